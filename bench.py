@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark: site-updates/s of the plain 2D Cellular Potts sweep at 4096^2.
+
+Workload (the reference's scaling configuration at its largest plane): a
+periodic 4096 x 4096 int32 lattice tiled by 262,144 square cells of side 8,
+one cell type, Moore contact J = 10, lambda_V = 1 with V_target = 64,
+lambda_S = 0.2 with S_target = 92 (an 8 x 8 square's initial unlike-bond
+count), T = 10, counter-hash RNG from seed 1. Synthetic: the lattice is the
+tiling itself, as the reference's bench builds it (glazier/examples/bench.rs).
+
+One timed step is one Monte Carlo step (16.8 M site updates). `value` is
+device time (CUDA events on the engine's stream), inputs resident in HBM,
+L2 flushed by a 256 MB write between timed steps. `e2e` runs whole jobs
+through the public API from pinned host memory: upload the lattice
+(glz_gpu_set_labels), 100 MCS (glz_gpu_step), download it (glz_gpu_labels).
+
+`--impl reference` times the reference's serial engine (its C restatement,
+pinned bit for bit to the reference's compiled module) on the host cores,
+one independent replica per core.
+
+Multi-GPU: replicas only. Under torchrun each rank runs its own lattice
+with no exchange; value is all ranks' site updates over the slowest rank.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PUBLISHED_4096 = 3.76e9  # README.md:121 of the reference: 4096^2, 100 MCS in 0.446 s (RTX 5060 Laptop)
+FALLBACK_HBM_GBS = 6650.0
+BYTES_PER_SITE_UPDATE = 20  # 4 colour passes x 4 B label read + 4 B label write per site per MCS
+METRIC = "site-updates/s (plain 2D sweep, 4096^2)"
+
+
+def workload(size: int):
+    from glazier_b200.blueprint import CellType, Model, Start
+
+    model = Model(
+        width=size,
+        height=size,
+        contact=[0.0, 10.0, 10.0, 10.0],
+        types=[CellType(), CellType(target_volume=64.0, lambda_volume=1.0, target_surface=92.0, lambda_surface=0.2)],
+        temperature=10.0,
+        neighbour_order=2,
+        seed=1,
+    )
+    return Start.tiled(model, 8)
+
+
+def config_dict(size: int, n: int) -> dict:
+    return {
+        "workload": f"plain 2D monolayer {size}x{size}, {(size // 8) ** 2} cells of side 8, Moore J=10, "
+                    "lambda_V=1 V_t=64, lambda_S=0.2 S_t=92, T=10, seed 1",
+        "sites": size * size,
+        "step": "one Monte Carlo step (sites copy attempts, 4 colour passes)",
+        "l2": "flushed between timed steps (256 MB write); the lattice is 64 MB",
+        "parallelism": f"replicas x{n}" if n > 1 else "single replica",
+        "e2e_step": "one job: upload lattice from pinned host, 100 MCS, download lattice",
+        "baseline_note": "vs_baseline divides by the reference README's 4096^2 device figure (RTX 5060 Laptop, "
+                         "bench.rs model J=[0,16,16,8], lambda_V=2, no surface term)",
+    }
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self) -> dict:
+        rows = []
+        for line in (self.out or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, flags in rows for k, f in enumerate(flags) if f.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak() -> tuple:
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        peaks = json.loads(path.read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+    path = ROOT / "profiles" / "sweep_2d_4096.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(size: int, seconds: float) -> dict:
+    """The serial engine on one host core, a bounded sample of the same lattice."""
+    from oracle.serial import SerialOracle
+
+    start = workload(size)
+    o = SerialOracle.from_start(start)
+    o.attempts(200_000)  # warm
+    t = time.perf_counter()
+    probe = 2_000_000
+    o.attempts(probe)
+    rate = probe / (time.perf_counter() - t)
+    n = max(probe, int(rate * seconds))
+    t = time.perf_counter()
+    o.attempts(n)
+    dt = time.perf_counter() - t
+    return {"value": n / dt, "unit": "site-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{n} serial copy attempts ({n / start.model.sites:.2f} MCS) on the {size}^2 lattice, "
+                      "C restatement of glazier-core/src/cpu.rs pinned bit-exact to the reference module"}
+
+
+def _reference_worker(args):
+    size, per_step, steps, warmup = args
+    sys.path.insert(0, str(ROOT))
+    from oracle.serial import SerialOracle
+
+    o = SerialOracle.from_start(workload(size))
+    for _ in range(warmup):
+        o.attempts(per_step)
+    t = time.perf_counter()
+    for _ in range(steps):
+        o.attempts(per_step)
+    return time.perf_counter() - t
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    from oracle import build as obuild
+
+    obuild.build()
+    # calibrate: a step is about half a second of one core's work
+    from oracle.serial import SerialOracle
+
+    o = SerialOracle.from_start(workload(args.size))
+    t = time.perf_counter()
+    o.attempts(1_000_000)
+    rate = 1_000_000 / (time.perf_counter() - t)
+    del o
+    per_step = max(100_000, int(rate * 0.5))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        times = pool.map(_reference_worker, [(args.size, per_step, args.steps, args.warmup)] * cores)
+    wall = max(times)
+    total = per_step * args.steps * cores
+    value = total / wall
+    line = {
+        "metric": METRIC, "value": value, "unit": "site-updates/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args.size, args.gpus),
+        "cpu_baseline": {"value": value, "unit": "site-updates/s", "cores": cores, "kind": "port",
+                         "sample": f"{cores} independent serial replicas, {per_step} copy attempts per step each"},
+        "e2e": {"value": value, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from glazier_b200.engine import GpuSimulation
+
+    start = workload(args.size)
+    sites = start.model.sites
+    sim = GpuSimulation.from_start(start, device=torch.cuda.current_device())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)  # 256 MB, past the 126 MB L2
+
+    sim.step(args.warmup)
+    phys = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    smi_index = int(phys[local]) if len(phys) > local and phys[local].strip().isdigit() else local
+    sweep_ms = field_ms = pop_ms = 0.0
+    barrier()
+    with Clocks(smi_index) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s, f, p = sim.step_profiled(1)
+            sweep_ms += s
+            field_ms += f
+            pop_ms += p
+        barrier()
+    total_ms = sweep_ms + field_ms + pop_ms
+    slowest = max_over_ranks(total_ms)
+    value = sites * args.steps * world / (slowest / 1e3)
+    launches_per_step = 4  # four colour passes; the workload has no fields and no population
+
+    # end to end through the public API, host buffers pinned
+    pinned_in = torch.from_numpy(start.labels.view(np.int32)).pin_memory()
+    pinned_out = torch.empty(sites, dtype=torch.int32).pin_memory()
+    jobs, job_mcs = args.e2e_jobs, 100
+    sim.set_labels_from(pinned_in.data_ptr(), sites)
+    sim.step(1)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(jobs):
+        sim.set_labels_from(pinned_in.data_ptr(), sites)
+        sim.step(job_mcs)
+        sim.labels_to(pinned_out.data_ptr(), sites)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = sites * job_mcs * jobs * world / e2e_s
+    assert int(pinned_out.max()) <= (args.size // 8) ** 2
+
+    peak, peak_kind = measured_peak()
+    launch_s = (sweep_ms / 1e3) / (args.steps * launches_per_step)
+    bytes_per_launch = sites * BYTES_PER_SITE_UPDATE / 4
+    achieved = bytes_per_launch / launch_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": committed_traffic(), "peak_source": peak_kind,
+                "kernel": "sweep_kernel<2,8> (one colour pass)",
+                "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3}
+
+    sim.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": value / world / PUBLISHED_4096, "dtype": "f32", "data": "synthetic",
+        "config": config_dict(args.size, world),
+        "e2e": {"value": e2e_value, "unit": "site-updates/s", "h2d_bytes_per_step": sites * 4,
+                "d2h_bytes_per_step": sites * 4, "jobs": jobs, "mcs_per_job": job_mcs},
+        "roofline": roofline,
+        "gpu_launches": args.steps * launches_per_step,
+        "clocks": clocks.summary(),
+        "phase_ms": {"sweep": sweep_ms, "fields": field_ms, "population": pop_ms},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.size, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--e2e-jobs", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

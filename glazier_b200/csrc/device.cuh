@@ -1,0 +1,93 @@
+// Device helpers shared by the sweep, field and population kernels.
+//
+// The counter hash is the reference device engine's (glazier-cuda/src/lib.rs
+// 33-50): SplitMix64's finaliser over seed ^ C1*site ^ C2*step ^ C3*stream.
+// The step and stream parts are the same for every thread of a launch, so the
+// host folds them into one 64-bit word per stream and a draw costs one
+// 64x32-bit multiply plus the finaliser.
+#pragma once
+
+#include <cstdint>
+
+namespace glz {
+
+constexpr uint64_t kSiteMul = 0xD1B54A32D192ED03ULL;
+constexpr uint64_t kStepMul = 0xA0761D6478BD642FULL;
+constexpr uint64_t kStreamMul = 0xE7037ED1A0B428DBULL;
+
+// The population step's draws take stream index 4*16, clear of the sweep's
+// 4*colour + {0, 1} for colours 0..7.
+constexpr int kPopulationStream = 16;
+
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// seed ^ C2*step ^ C3*(4*colour + index): the launch-uniform part of a draw.
+__host__ __device__ __forceinline__ uint64_t stream_key(uint64_t seed, int32_t step, int colour, int index) {
+    return seed ^ (kStepMul * (uint64_t)(int64_t)step) ^ (kStreamMul * (uint64_t)(int64_t)(4 * colour + index));
+}
+
+__host__ __device__ __forceinline__ uint64_t draw(uint64_t key, uint32_t site) {
+    return mix64(key ^ (kSiteMul * (uint64_t)site));
+}
+
+// (bits >> 11) * 2^-53 rounded to f32: the reference computes the product in
+// f64 and rounds once (lib.rs:48-50); rounding the 53-bit integer to f32 and
+// scaling by a power of two rounds the same value once, so the bits agree.
+__device__ __forceinline__ float to_f32(uint64_t bits) { return __ull2float_rn(bits >> 11) * 0x1p-53f; }
+
+__device__ __forceinline__ double to_f64(uint64_t bits) { return __ull2double_rn(bits >> 11) * 0x1p-53; }
+
+// exp for the Metropolis test, written from Cody and Waite's method (W. J.
+// Cody, W. Waite, "Software Manual for the Elementary Functions", 1980):
+// k = rint(x log2 e), r = x - k ln2 with ln 2 split hi + lo, e^r by the
+// degree-7 Taylor polynomial in fused multiply-adds, scaled by 2^k through the
+// exponent field. Only correctly rounded operations, so a host replay gets the
+// same bits. Below -87 the result is zero: no draw in [0, 1) falls under it.
+__device__ __forceinline__ float metropolis_exp(float x) {
+    if (x < -87.0f) return 0.0f;
+    if (x > 88.0f) return __int_as_float(0x7f800000);
+    float k = rintf(__fmul_rn(x, 1.44269504088896341f));
+    float r = __fmaf_rn(k, -0.693145751953125f, x);
+    r = __fmaf_rn(k, -1.428606765330187e-06f, r);
+    float p = 1.98412698e-04f;
+    p = __fmaf_rn(p, r, 1.38888889e-03f);
+    p = __fmaf_rn(p, r, 8.33333333e-03f);
+    p = __fmaf_rn(p, r, 4.16666667e-02f);
+    p = __fmaf_rn(p, r, 1.66666667e-01f);
+    p = __fmaf_rn(p, r, 0.5f);
+    p = __fmaf_rn(p, r, 1.0f);
+    p = __fmaf_rn(p, r, 1.0f);
+    int ki = (int)k;
+    return __fmul_rn(p, __int_as_float((ki + 127) << 23));
+}
+
+__host__ __device__ __forceinline__ int wrap(int v, int n) {
+    int r = v % n;
+    return r < 0 ? r + n : r;
+}
+
+// Minimum image of an integer offset on a periodic axis (moments.rs:36-46).
+__host__ __device__ __forceinline__ int fold_int(int d, int span) {
+    if (2 * d > span) return d - span;
+    if (2 * d < -span) return d + span;
+    return d;
+}
+
+// Per-cell (volume, surface) deltas packed in one 64-bit word so a commit is
+// one atomic: the word holds surface * 2^32 + volume modulo 2^64, and a
+// volume delta below 2^31 in size decodes exactly.
+__device__ __forceinline__ unsigned long long pack_delta(int dv, int ds) {
+    return ((unsigned long long)(long long)ds << 32) + (unsigned long long)(long long)dv;
+}
+
+__host__ __device__ __forceinline__ void unpack_delta(long long p, int &dv, int &ds) {
+    dv = (int)(uint32_t)(uint64_t)p;
+    ds = (int)((p - (long long)dv) >> 32);
+}
+
+}  // namespace glz

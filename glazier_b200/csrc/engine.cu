@@ -1,0 +1,748 @@
+// The host engine behind the C ABI in include/glazier_gpu.h.
+//
+// Replaces `GpuSimulation` (glazier-cuda/src/lib.rs:748-1533): it owns the
+// device copy of a run, one CUDA stream, and the per-step schedule
+//   sweep colour 0 .. ncol-1  ->  field rounds  ->  division and death
+// (lib.rs:1075-1141). Kernels are compiled ahead of time for sm_100a; there
+// is no run-time compilation and no CPU path: a call that cannot run on the
+// device fails with a status.
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/glazier_gpu.h"
+#include "device.cuh"
+#include "engine.h"
+
+namespace glz {
+int sweep_box(int dim, uint32_t box[3]);
+}
+
+namespace {
+
+thread_local std::string g_error = "no error";
+
+int fail(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+#define CU(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) return fail(GLZ_DRIVER, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// lattice.rs:8-88: the neighbour offsets of an order, in the reference's
+// order (the sweep's pick and the contact sum both follow it).
+int offsets_for(int order, int depth, int out[26][3]) {
+    static const int O1[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    static const int O2[18][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  {0, -1, 0}, {0, 0, 1},  {0, 0, -1},
+                                  {1, 1, 0},  {1, -1, 0}, {-1, 1, 0}, {-1, -1, 0}, {1, 0, 1}, {1, 0, -1},
+                                  {-1, 0, 1}, {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1}, {0, -1, -1}};
+    int all[26][3];
+    int k = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+                if (dx || dy || dz) {
+                    all[k][0] = dx;
+                    all[k][1] = dy;
+                    all[k][2] = dz;
+                    ++k;
+                }
+    int n = 0;
+    if (depth > 1) {
+        if (order == 1) {
+            std::memcpy(out, O1, sizeof O1);
+            return 6;
+        }
+        if (order == 2) {
+            std::memcpy(out, O2, sizeof O2);
+            return 18;
+        }
+        std::memcpy(out, all, sizeof all);
+        return 26;
+    }
+    if (order >= 2) {
+        for (int i = 0; i < 26; ++i)
+            if (all[i][2] == 0) std::memcpy(out[n++], all[i], sizeof all[i]);
+        return n;
+    }
+    for (int i = 0; i < 6; ++i)
+        if (O1[i][2] == 0) std::memcpy(out[n++], O1[i], sizeof O1[i]);
+    return n;
+}
+
+// field.rs:155-160
+int substeps_for(double diffusion, int dimensions) {
+    if (diffusion <= 0.0) return 1;
+    double k = std::ceil(diffusion / (1.0 / (2.0 * (double)dimensions)));
+    return k < 1.0 ? 1 : (int)k;
+}
+
+double at(const double *p, size_t i) { return p ? p[i] : 0.0; }
+
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+}  // namespace
+
+struct glz_gpu {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    glz::Geometry g{};
+    int n_types = 0, n_species = 0;
+    float temperature = 0.0f;
+    uint64_t seed = 0;
+    bool has_length = false, tracks = false, has_chemotaxis = false, has_pop = false;
+    int substeps[glz::kMaxSpecies] = {};
+    float fd[glz::kMaxSpecies] = {}, fdecay[glz::kMaxSpecies] = {};
+
+    // per-type tables
+    float *contact = nullptr, *tv = nullptr, *lv = nullptr, *ts = nullptr, *ls = nullptr;
+    float *chemo = nullptr, *sec = nullptr, *upt = nullptr;
+    double *tl = nullptr, *ll = nullptr, *divv = nullptr, *death = nullptr;
+    uint8_t *connected = nullptr;
+
+    // state
+    uint32_t *labels = nullptr;
+    uint8_t *cell_type = nullptr;
+    std::vector<uint8_t> cell_type_host;
+    size_t n_labels = 0, cap = 0;
+    glz::Tallies t{};
+    float *field_buf = nullptr;  // 2 * n_species * sites: two buffers per species
+    int field_cur[glz::kMaxSpecies] = {};
+    uint64_t pass_no = 0, mcs = 0;
+    bool use_tma = false;
+    CUtensorMap tmap{};
+    int *error_flag = nullptr;
+    unsigned long long *medium = nullptr;
+
+    // population scratch, `cap` entries each
+    unsigned char *mode = nullptr;
+    double *plan = nullptr;
+    int *moved = nullptr;
+    uint32_t *daughter = nullptr;
+    int *counters = nullptr;
+
+    float *field_ptr(int s, int which) { return field_buf + ((size_t)2 * s + which) * (size_t)g.sites; }
+
+    glz::TypeTables tables() const {
+        glz::TypeTables tt{};
+        tt.contact = contact;
+        tt.target_volume = tv;
+        tt.lambda_volume = lv;
+        tt.target_surface = ts;
+        tt.lambda_surface = ls;
+        tt.target_length = tl;
+        tt.lambda_length = ll;
+        tt.division_volume = divv;
+        tt.death_rate = death;
+        tt.connected = connected;
+        tt.chemotaxis = chemo;
+        tt.secretion = sec;
+        tt.uptake = upt;
+        return tt;
+    }
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(T **p, size_t n) {
+    CU(cudaMalloc((void **)p, (n ? n : 1) * sizeof(T)));
+    return GLZ_OK;
+}
+
+template <typename T>
+int upload(glz_gpu *h, T **p, const std::vector<T> &host) {
+    int rc = dev_alloc(p, host.size());
+    if (rc) return rc;
+    if (!host.empty()) CU(cudaMemcpyAsync(*p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    return GLZ_OK;
+}
+
+void free_tallies(glz::Tallies &t) {
+    for (auto *p : t.vs_base) cudaFree(p);
+    for (auto *p : t.vs_delta) cudaFree(p);
+    for (auto *p : t.mom_base) cudaFree(p);
+    for (auto *p : t.mom_delta) cudaFree(p);
+    cudaFree(t.vol_by_colour);
+    cudaFree(t.anchor);
+    t = glz::Tallies{};
+}
+
+void free_population(glz_gpu *h) {
+    cudaFree(h->mode);
+    cudaFree(h->plan);
+    cudaFree(h->moved);
+    cudaFree(h->daughter);
+    h->mode = nullptr;
+    h->plan = nullptr;
+    h->moved = nullptr;
+    h->daughter = nullptr;
+}
+
+// Per-label arrays sized for `cap` labels. The settled tallies, anchors,
+// per-colour volumes and cell types of the first n_labels entries carry over
+// exactly, so growing never changes a run; every delta word starts at zero.
+int alloc_labels(glz_gpu *h, size_t cap) {
+    const int nm = h->g.nm;
+    const size_t n = h->n_labels;
+    const uint64_t p = h->pass_no;
+    glz::Tallies fresh{};
+    for (int k = 0; k < 2; ++k) {
+        if (int rc = dev_alloc(&fresh.vs_base[k], cap)) return rc;
+        if (h->tracks)
+            if (int rc = dev_alloc(&fresh.mom_base[k], cap * nm)) return rc;
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (int rc = dev_alloc(&fresh.vs_delta[k], cap)) return rc;
+        CU(cudaMemsetAsync(fresh.vs_delta[k], 0, cap * sizeof(long long), h->stream));
+        if (h->tracks) {
+            if (int rc = dev_alloc(&fresh.mom_delta[k], cap * nm)) return rc;
+            CU(cudaMemsetAsync(fresh.mom_delta[k], 0, cap * nm * sizeof(long long), h->stream));
+        }
+    }
+    if (int rc = dev_alloc(&fresh.vol_by_colour, cap * h->g.ncol)) return rc;
+    if (int rc = dev_alloc(&fresh.anchor, cap * 4)) return rc;
+    uint8_t *types = nullptr;
+    if (int rc = dev_alloc(&types, cap)) return rc;
+    if (n) CU(cudaMemcpyAsync(types, h->cell_type_host.data(), n, cudaMemcpyHostToDevice, h->stream));
+    if (h->cap) {
+        // the caller has settled: base slot p % 2 holds every tally
+        CU(cudaMemcpyAsync(fresh.vs_base[p % 2], h->t.vs_base[p % 2], n * sizeof(int2), cudaMemcpyDeviceToDevice,
+                           h->stream));
+        if (h->tracks)
+            CU(cudaMemcpyAsync(fresh.mom_base[p % 2], h->t.mom_base[p % 2], n * nm * sizeof(long long),
+                               cudaMemcpyDeviceToDevice, h->stream));
+        CU(cudaMemcpyAsync(fresh.vol_by_colour, h->t.vol_by_colour, n * h->g.ncol * sizeof(int),
+                           cudaMemcpyDeviceToDevice, h->stream));
+        CU(cudaMemcpyAsync(fresh.anchor, h->t.anchor, n * 4 * sizeof(int), cudaMemcpyDeviceToDevice, h->stream));
+    }
+    CU(cudaStreamSynchronize(h->stream));
+    free_tallies(h->t);
+    h->t = fresh;
+    free_population(h);
+    if (h->has_pop) {
+        if (int rc = dev_alloc(&h->mode, cap)) return rc;
+        if (int rc = dev_alloc(&h->plan, cap * 6)) return rc;
+        if (int rc = dev_alloc(&h->moved, cap)) return rc;
+        if (int rc = dev_alloc(&h->daughter, cap)) return rc;
+    }
+    cudaFree(h->cell_type);
+    h->cell_type = types;
+    h->cap = cap;
+    return GLZ_OK;
+}
+
+int recount(glz_gpu *h) {
+    const uint64_t p = h->pass_no;
+    glz::RecountLaunch r{};
+    r.g = h->g;
+    r.labels = h->labels;
+    r.n_labels = (int)h->n_labels;
+    r.vs_base = h->t.vs_base[p % 2];
+    r.mom_base = h->t.mom_base[p % 2];
+    for (int k = 0; k < 3; ++k) {
+        r.vs_delta[k] = h->t.vs_delta[k];
+        r.mom_delta[k] = h->t.mom_delta[k];
+    }
+    r.vol_by_colour = h->t.vol_by_colour;
+    r.anchor = h->t.anchor;
+    r.tracks = h->tracks;
+    r.error_flag = h->error_flag;
+    CU(glz::launch_recount(r, h->stream));
+    return GLZ_OK;
+}
+
+int settle(glz_gpu *h) {
+    const uint64_t p = h->pass_no;
+    CU(glz::launch_settle(h->t.vs_base[p % 2], h->t.vs_delta[(p + 2) % 3], h->t.mom_base[p % 2],
+                          h->t.mom_delta[(p + 2) % 3], h->g.nm, (int)h->n_labels, h->tracks, h->stream));
+    return GLZ_OK;
+}
+
+int sweep_pass(glz_gpu *h, int colour) {
+    const uint64_t p = h->pass_no;
+    glz::SweepLaunch a{};
+    a.g = h->g;
+    a.t = h->tables();
+    a.n_types = h->n_types;
+    a.n_species = h->n_species;
+    a.temperature = h->temperature;
+    a.colour = colour;
+    a.step = (int32_t)h->mcs;
+    a.key_pick = glz::stream_key(h->seed, a.step, colour, 0);
+    a.key_accept = glz::stream_key(h->seed, a.step, colour, 1);
+    a.labels = h->labels;
+    a.cell_type = h->cell_type;
+    a.vs_base = h->t.vs_base[p % 2];
+    a.vs_prev = h->t.vs_delta[(p + 2) % 3];
+    a.vs_cur = reinterpret_cast<unsigned long long *>(h->t.vs_delta[p % 3]);
+    a.vs_next_base = h->t.vs_base[(p + 1) % 2];
+    a.vs_clear = h->t.vs_delta[(p + 1) % 3];
+    a.mom_base = h->t.mom_base[p % 2];
+    a.mom_prev = h->t.mom_delta[(p + 2) % 3];
+    a.mom_cur = reinterpret_cast<unsigned long long *>(h->t.mom_delta[p % 3]);
+    a.mom_next_base = h->t.mom_base[(p + 1) % 2];
+    a.mom_clear = h->t.mom_delta[(p + 1) % 3];
+    a.vol_by_colour = h->t.vol_by_colour;
+    a.anchor = h->t.anchor;
+    a.n_labels = (int)h->n_labels;
+    a.has_length = h->has_length;
+    a.tracks = h->tracks;
+    a.has_chemotaxis = h->has_chemotaxis;
+    for (int s = 0; s < h->n_species; ++s) a.fields[s] = h->field_ptr(s, h->field_cur[s]);
+    a.use_tma = h->use_tma;
+    a.tensor_map = h->use_tma ? &h->tmap : nullptr;
+    a.error_flag = h->error_flag;
+    CU(glz::launch_sweep(a, h->stream));
+    h->pass_no += 1;
+    return GLZ_OK;
+}
+
+int field_step(glz_gpu *h) {
+    int rounds = 0;
+    for (int s = 0; s < h->n_species; ++s) rounds = h->substeps[s] > rounds ? h->substeps[s] : rounds;
+    for (int r = 0; r < rounds; ++r) {
+        glz::FieldLaunch f{};
+        f.g = h->g;
+        f.n_species = h->n_species;
+        f.round = r;
+        f.labels = h->labels;
+        f.cell_type = h->cell_type;
+        f.secretion = h->sec;
+        f.uptake = h->upt;
+        for (int s = 0; s < h->n_species; ++s) {
+            f.active[s] = r < h->substeps[s];
+            f.last[s] = r == h->substeps[s] - 1;
+            f.d[s] = h->fd[s];
+            f.decay[s] = h->fdecay[s];
+            f.in[s] = h->field_ptr(s, h->field_cur[s]);
+            f.out[s] = h->field_ptr(s, 1 - h->field_cur[s]);
+        }
+        CU(glz::launch_field_round(f, h->stream));
+        for (int s = 0; s < h->n_species; ++s)
+            if (f.active[s]) h->field_cur[s] = 1 - h->field_cur[s];
+    }
+    return GLZ_OK;
+}
+
+// Keep room for every cell to divide once: the most one step can add.
+int ensure_capacity(glz_gpu *h) {
+    if (h->cap >= 2 * h->n_labels) return GLZ_OK;
+    if (int rc = settle(h)) return rc;
+    return alloc_labels(h, 4 * h->n_labels);
+}
+
+int population(glz_gpu *h) {
+    if (int rc = ensure_capacity(h)) return rc;
+    if (int rc = settle(h)) return rc;
+    const uint64_t p = h->pass_no;
+    glz::PopulationLaunch a{};
+    a.g = h->g;
+    a.t = h->tables();
+    a.labels = h->labels;
+    a.cell_type_in = h->cell_type;
+    a.cell_type_out = h->cell_type;
+    a.n_labels = (int)h->n_labels;
+    a.cap = (int)h->cap;
+    a.vs_base = h->t.vs_base[p % 2];
+    a.mom_base = h->t.mom_base[p % 2];
+    a.anchor = h->t.anchor;
+    a.key_death = glz::stream_key(h->seed, (int32_t)h->mcs, glz::kPopulationStream, 0);
+    a.mode = h->mode;
+    a.plan = h->plan;
+    a.moved = h->moved;
+    a.daughter = h->daughter;
+    a.counters = h->counters;
+    CU(glz::launch_population_plan(a, h->stream));
+    int counters[2] = {0, 0};
+    CU(cudaMemcpyAsync(counters, h->counters, sizeof counters, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (!counters[1]) return GLZ_OK;
+    CU(glz::launch_population_apply(a, h->stream));
+    const size_t born = (size_t)counters[0];
+    if (born) {
+        h->cell_type_host.resize(h->n_labels + born);
+        CU(cudaMemcpyAsync(h->cell_type_host.data() + h->n_labels, h->cell_type + h->n_labels, born,
+                           cudaMemcpyDeviceToHost, h->stream));
+        h->n_labels += born;
+    }
+    if (int rc = recount(h)) return rc;
+    CU(cudaStreamSynchronize(h->stream));
+    return GLZ_OK;
+}
+
+int check_error_flag(glz_gpu *h) {
+    int flag = 0;
+    CU(cudaMemcpyAsync(&flag, h->error_flag, sizeof flag, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (flag == 1) return fail(GLZ_DRIVER, "a sweep tile's tensor copy did not complete within its wait limit");
+    if (flag == 2) return fail(GLZ_INVALID, "a label is not below the cell type count");
+    return GLZ_OK;
+}
+
+// The step schedule, with each phase bracketed by events when `ms` is given.
+int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
+    cudaEvent_t ev[6] = {};
+    if (ms) {
+        for (auto &e : ev) CU(cudaEventCreate(&e));
+        ms[0] = ms[1] = ms[2] = 0.0;
+    }
+    int rc = GLZ_OK;
+    for (uint64_t r = 0; r < steps && rc == GLZ_OK; ++r) {
+        if (ms) CU(cudaEventRecord(ev[0], h->stream));
+        for (int c = 0; c < h->g.ncol && rc == GLZ_OK; ++c) rc = sweep_pass(h, c);
+        if (ms) CU(cudaEventRecord(ev[1], h->stream));
+        if (rc == GLZ_OK && h->n_species > 0) rc = field_step(h);
+        if (ms) CU(cudaEventRecord(ev[2], h->stream));
+        if (rc == GLZ_OK && h->has_pop) rc = population(h);
+        if (ms) CU(cudaEventRecord(ev[3], h->stream));
+        h->mcs += 1;
+        if (ms && rc == GLZ_OK) {
+            CU(cudaEventSynchronize(ev[3]));
+            for (int k = 0; k < 3; ++k) {
+                float t = 0.0f;
+                CU(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+                ms[k] += t;
+            }
+        }
+    }
+    if (ms)
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    if (rc != GLZ_OK) return rc;
+    CU(cudaStreamSynchronize(h->stream));
+    return check_error_flag(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *glz_last_error(void) { return g_error.c_str(); }
+
+int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *cell_type, size_t n_labels,
+                   const double *fields, const double *activity, glz_gpu **out) {
+    if (!out) return fail(GLZ_INVALID, "null output handle");
+    *out = nullptr;
+    if (!m || !labels || !cell_type) return fail(GLZ_INVALID, "null model, labels or cell types");
+    const int w = m->width, hh = m->height, d = m->depth;
+    if (w <= 0 || hh <= 0 || d <= 0) return fail(GLZ_INVALID, "the lattice has a zero dimension");
+    if (w % 2 != 0 || hh % 2 != 0 || (d > 1 && d % 2 != 0)) {
+        char msg[160];
+        std::snprintf(msg, sizeof msg, "the checkerboard split needs even sides; the lattice is %d by %d by %d", w, hh,
+                      d);
+        return fail(GLZ_ODD_LATTICE, msg);
+    }
+    const long long sites = (long long)w * hh * d;
+    if (sites >= (1LL << 31)) return fail(GLZ_INVALID, "the lattice has 2^31 sites or more");
+    const int nt = m->n_types, ns = m->n_species;
+    if (nt < 1 || nt > 255 || !m->contact) return fail(GLZ_INVALID, "the model needs 1 to 255 types and a contact matrix");
+    if (ns < 0 || ns > glz::kMaxSpecies) return fail(GLZ_INVALID, "the device engine runs at most 8 species");
+    if (m->neighbour_order < 1 || m->neighbour_order > 3)
+        return fail(GLZ_INVALID, "neighbour order is outside the range one to three");
+    if (!(m->temperature > 0.0)) return fail(GLZ_INVALID, "the temperature must be positive");
+    if (n_labels < 1) return fail(GLZ_INVALID, "the cell type table is empty");
+
+    bool nematic = false, motility = false, drift = false;
+    for (int k = 0; k < nt; ++k) {
+        nematic |= m->nematic && at(m->lambda_nematic, k) != 0.0;
+        motility |= at(m->lambda_activity, k) != 0.0 && at(m->max_activity, k) > 0.0;
+        for (int a = 0; a < 3; ++a) drift |= at(m->external, 3 * (size_t)k + a) != 0.0;
+    }
+    if (nematic) return fail(GLZ_UNSUPPORTED, "the device engine does not run the nematic term");
+    if (motility) return fail(GLZ_UNSUPPORTED, "the device engine does not run the motility (Act) term");
+    if (drift) return fail(GLZ_UNSUPPORTED, "the device engine does not run the external drift term");
+    if (activity)
+        for (long long i = 0; i < sites; ++i)
+            if (activity[i] != 0.0) return fail(GLZ_UNSUPPORTED, "a nonzero activity needs the motility term");
+    for (long long i = 0; i < sites; ++i)
+        if (labels[i] >= n_labels) return fail(GLZ_INVALID, "a label is not below the cell type count");
+    for (size_t l = 0; l < n_labels; ++l)
+        if (cell_type[l] >= nt) return fail(GLZ_INVALID, "a cell type is not below the type count");
+
+    glz_gpu *h = new glz_gpu();
+    auto bail = [&](int rc) {
+        glz_gpu_destroy(h);
+        return rc;
+    };
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return bail(fail(GLZ_DRIVER, "no CUDA device"));
+    h->device = dev;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(GLZ_DRIVER, "cannot create a stream"));
+
+    glz::Geometry &g = h->g;
+    g.w = w;
+    g.h = hh;
+    g.d = d;
+    g.dim = d > 1 ? 3 : 2;
+    g.ncol = g.dim == 3 ? 8 : 4;
+    g.sites = (int)sites;
+    g.nm = g.dim == 3 ? 9 : 5;
+    g.n_off = offsets_for(m->neighbour_order, d, g.off);
+    h->n_types = nt;
+    h->n_species = ns;
+    h->temperature = (float)m->temperature;
+    h->seed = m->seed;
+
+    std::vector<float> contact(nt * nt), tv(nt), lv(nt), ts(nt), ls(nt);
+    std::vector<double> tl(nt), ll(nt), divv(nt), death(nt);
+    std::vector<uint8_t> conn(nt);
+    bool has_conn = false;
+    for (int a = 0; a < nt * nt; ++a) contact[a] = (float)m->contact[a];
+    for (int k = 0; k < nt; ++k) {
+        tv[k] = (float)at(m->target_volume, k);
+        lv[k] = (float)at(m->lambda_volume, k);
+        ts[k] = (float)at(m->target_surface, k);
+        ls[k] = (float)at(m->lambda_surface, k);
+        tl[k] = at(m->target_length, k);
+        ll[k] = at(m->lambda_length, k);
+        divv[k] = at(m->division_volume, k);
+        death[k] = at(m->death_rate, k);
+        conn[k] = m->connected ? (m->connected[k] != 0) : 0;
+        has_conn |= conn[k] != 0;
+        h->has_length |= ll[k] != 0.0;
+        h->has_pop |= divv[k] > 0.0 || death[k] > 0.0;
+    }
+    h->tracks = h->has_length || h->has_pop;
+    std::vector<float> chemo(nt * (size_t)ns), sec(nt * (size_t)ns), upt(nt * (size_t)ns);
+    for (size_t i = 0; i < chemo.size(); ++i) {
+        chemo[i] = (float)at(m->chemotaxis, i);
+        sec[i] = (float)at(m->secretion, i);
+        upt[i] = (float)at(m->uptake, i);
+        h->has_chemotaxis |= chemo[i] != 0.0f;
+    }
+    for (int s = 0; s < ns; ++s) {
+        h->substeps[s] = substeps_for(at(m->diffusion, s), g.dim);
+        h->fd[s] = (float)(at(m->diffusion, s) / (double)h->substeps[s]);
+        h->fdecay[s] = (float)(at(m->decay, s) / (double)h->substeps[s]);
+    }
+    if (has_conn) {
+        int all[26][3];
+        int n = offsets_for(3, d, all);  // the full Moore / 26 ring (connectivity.rs:23-29)
+        g.ring_n = n;
+        std::memcpy(g.ring, all, sizeof all);
+        for (int a = 0; a < n; ++a) {
+            uint32_t mask = 0;
+            for (int b = 0; b < n; ++b)
+                if (std::abs(all[a][0] - all[b][0]) <= 1 && std::abs(all[a][1] - all[b][1]) <= 1 &&
+                    std::abs(all[a][2] - all[b][2]) <= 1)
+                    mask |= 1u << b;
+            g.adjacency[a] = mask;
+        }
+    }
+
+    int rc;
+    if ((rc = upload(h, &h->contact, contact)) || (rc = upload(h, &h->tv, tv)) || (rc = upload(h, &h->lv, lv)) ||
+        (rc = upload(h, &h->ts, ts)) || (rc = upload(h, &h->ls, ls)) || (rc = upload(h, &h->tl, tl)) ||
+        (rc = upload(h, &h->ll, ll)) || (rc = upload(h, &h->divv, divv)) || (rc = upload(h, &h->death, death)) ||
+        (rc = upload(h, &h->connected, conn)) || (rc = upload(h, &h->chemo, chemo)) || (rc = upload(h, &h->sec, sec)) ||
+        (rc = upload(h, &h->upt, upt)))
+        return bail(rc);
+
+    if ((rc = dev_alloc(&h->labels, (size_t)sites))) return bail(rc);
+    if (cudaMemcpyAsync(h->labels, labels, sites * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream))
+        return bail(fail(GLZ_DRIVER, "label upload failed"));
+    h->cell_type_host.assign(cell_type, cell_type + n_labels);
+    h->n_labels = n_labels;
+    if ((rc = alloc_labels(h, h->has_pop ? 2 * n_labels + 16 : n_labels))) return bail(rc);
+
+    if (ns > 0) {
+        if ((rc = dev_alloc(&h->field_buf, (size_t)2 * ns * sites))) return bail(rc);
+        std::vector<float> f((size_t)sites);
+        for (int s = 0; s < ns; ++s) {
+            for (long long i = 0; i < sites; ++i) f[i] = (float)(fields ? fields[(size_t)s * sites + i] : at(m->initial, s));
+            if (cudaMemcpy(h->field_ptr(s, 0), f.data(), sites * sizeof(float), cudaMemcpyHostToDevice))
+                return bail(fail(GLZ_DRIVER, "field upload failed"));
+        }
+    }
+    if ((rc = dev_alloc(&h->error_flag, 1))) return bail(rc);
+    if ((rc = dev_alloc(&h->medium, 2))) return bail(rc);
+    if ((rc = dev_alloc(&h->counters, 2))) return bail(rc);
+    if (cudaMemsetAsync(h->error_flag, 0, sizeof(int), h->stream)) return bail(fail(GLZ_DRIVER, "memset failed"));
+
+    // The tensor copy needs rows that are a whole number of 16-byte units.
+    const char *env = std::getenv("GLAZIER_SWEEP_TMA");
+    h->use_tma = (w % 4 == 0) && !(env && env[0] == '0');
+    if (h->use_tma) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+            q != cudaDriverEntryPointSuccess) {
+            h->use_tma = false;
+        } else {
+            uint32_t box[3];
+            glz::sweep_box(g.dim, box);
+            const cuuint32_t rank = g.dim;
+            cuuint64_t dims[3] = {(cuuint64_t)w, (cuuint64_t)hh, (cuuint64_t)d};
+            cuuint64_t strides[2] = {(cuuint64_t)w * 4, (cuuint64_t)w * hh * 4};
+            cuuint32_t boxd[3] = {box[0], box[1], box[2]};
+            cuuint32_t elem[3] = {1, 1, 1};
+            CUresult r = reinterpret_cast<EncodeTiled>(fn)(
+                &h->tmap, CU_TENSOR_MAP_DATA_TYPE_UINT32, rank, h->labels, dims, strides, boxd, elem,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return bail(fail(GLZ_DRIVER, "cuTensorMapEncodeTiled failed"));
+        }
+    }
+    if ((rc = recount(h))) return bail(rc);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return bail(fail(GLZ_DRIVER, std::string("setup: ") + cudaGetErrorString(cudaGetLastError())));
+    *out = h;
+    return GLZ_OK;
+}
+
+int glz_set_device(int ordinal) {
+    CU(cudaSetDevice(ordinal));
+    return GLZ_OK;
+}
+
+int glz_gpu_step(glz_gpu *h, uint64_t steps) {
+    if (!h) return fail(GLZ_INVALID, "null handle");
+    return run_steps(h, steps, nullptr);
+}
+
+int glz_gpu_step_profiled(glz_gpu *h, uint64_t steps, double ms[3]) {
+    if (!h || !ms) return fail(GLZ_INVALID, "null handle or output");
+    return run_steps(h, steps, ms);
+}
+
+int glz_gpu_set_labels(glz_gpu *h, const uint32_t *labels, size_t sites) {
+    if (!h || !labels) return fail(GLZ_INVALID, "null handle or labels");
+    if (sites != (size_t)h->g.sites) return fail(GLZ_INVALID, "the lattice is not one label per site");
+    CU(cudaMemcpyAsync(h->labels, labels, sites * sizeof(uint32_t), cudaMemcpyHostToDevice, h->stream));
+    return recount(h);
+}
+
+int glz_gpu_labels(glz_gpu *h, uint32_t *out, size_t sites) {
+    if (!h || !out) return fail(GLZ_INVALID, "null handle or buffer");
+    if (sites != (size_t)h->g.sites) return fail(GLZ_INVALID, "the buffer is not one label per site");
+    CU(cudaMemcpyAsync(out, h->labels, sites * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return GLZ_OK;
+}
+
+int glz_gpu_field(glz_gpu *h, int index, double *out, size_t sites) {
+    if (!h || !out) return fail(GLZ_INVALID, "null handle or buffer");
+    if (index < 0 || index >= h->n_species) return fail(GLZ_INVALID, "no such species");
+    if (sites != (size_t)h->g.sites) return fail(GLZ_INVALID, "the buffer is not one value per site");
+    std::vector<float> f(sites);
+    CU(cudaMemcpyAsync(f.data(), h->field_ptr(index, h->field_cur[index]), sites * sizeof(float),
+                       cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < sites; ++i) out[i] = (double)f[i];
+    return GLZ_OK;
+}
+
+static int read_tallies(glz_gpu *h, std::vector<int2> &vs, unsigned long long medium[2]) {
+    if (int rc = settle(h)) return rc;
+    vs.resize(h->n_labels);
+    CU(cudaMemcpyAsync(vs.data(), h->t.vs_base[h->pass_no % 2], h->n_labels * sizeof(int2), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(glz::launch_medium_count(h->g, h->labels, h->medium, h->stream));
+    CU(cudaMemcpyAsync(medium, h->medium, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return GLZ_OK;
+}
+
+int glz_gpu_volumes(glz_gpu *h, uint32_t *out, size_t *count) {
+    if (!h || !count) return fail(GLZ_INVALID, "null handle or count");
+    if (!out || *count < h->n_labels) {
+        *count = h->n_labels;
+        return fail(GLZ_INVALID, "the buffer is shorter than the label count");
+    }
+    std::vector<int2> vs;
+    unsigned long long medium[2];
+    if (int rc = read_tallies(h, vs, medium)) return rc;
+    out[0] = (uint32_t)medium[0];
+    for (size_t l = 1; l < h->n_labels; ++l) out[l] = vs[l].x > 0 ? (uint32_t)vs[l].x : 0u;
+    *count = h->n_labels;
+    return GLZ_OK;
+}
+
+int glz_gpu_surfaces(glz_gpu *h, int64_t *out, size_t *count) {
+    if (!h || !count) return fail(GLZ_INVALID, "null handle or count");
+    if (!out || *count < h->n_labels) {
+        *count = h->n_labels;
+        return fail(GLZ_INVALID, "the buffer is shorter than the label count");
+    }
+    std::vector<int2> vs;
+    unsigned long long medium[2];
+    if (int rc = read_tallies(h, vs, medium)) return rc;
+    out[0] = (int64_t)medium[1];
+    for (size_t l = 1; l < h->n_labels; ++l) out[l] = (int64_t)vs[l].y;
+    *count = h->n_labels;
+    return GLZ_OK;
+}
+
+int glz_gpu_cell_types(glz_gpu *h, uint8_t *out, size_t *count) {
+    if (!h || !count) return fail(GLZ_INVALID, "null handle or count");
+    if (!out || *count < h->n_labels) {
+        *count = h->n_labels;
+        return fail(GLZ_INVALID, "the buffer is shorter than the label count");
+    }
+    std::memcpy(out, h->cell_type_host.data(), h->n_labels);
+    *count = h->n_labels;
+    return GLZ_OK;
+}
+
+int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len) {
+    if (!h) return fail(GLZ_INVALID, "null handle");
+    if (len != 2 * (size_t)h->g.sites) {
+        char msg[128];
+        std::snprintf(msg, sizeof msg, "nematic field has %zu sites, the lattice %d", len / 2, h->g.sites);
+        return fail(GLZ_INVALID, msg);
+    }
+    (void)field;
+    // Models with a nematic coupling are refused at creation, so no handle
+    // has one to update (lib.rs:1207-1210).
+    return fail(GLZ_UNSUPPORTED, "the model has no nematic coupling to update");
+}
+
+uint64_t glz_gpu_mcs(const glz_gpu *h) { return h ? h->mcs : 0; }
+
+size_t glz_gpu_n_labels(const glz_gpu *h) { return h ? h->n_labels : 0; }
+
+void *glz_gpu_stream(glz_gpu *h) { return h ? (void *)h->stream : nullptr; }
+
+int glz_gpu_device_labels(glz_gpu *h, void **labels) {
+    if (!h || !labels) return fail(GLZ_INVALID, "null handle or output");
+    *labels = h->labels;
+    return GLZ_OK;
+}
+
+int glz_gpu_device_field(glz_gpu *h, int index, void **field) {
+    if (!h || !field) return fail(GLZ_INVALID, "null handle or output");
+    if (index < 0 || index >= h->n_species) return fail(GLZ_INVALID, "no such species");
+    *field = h->field_ptr(index, h->field_cur[index]);
+    return GLZ_OK;
+}
+
+void glz_gpu_destroy(glz_gpu *h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->contact); cudaFree(h->tv); cudaFree(h->lv); cudaFree(h->ts); cudaFree(h->ls);
+    cudaFree(h->chemo); cudaFree(h->sec); cudaFree(h->upt);
+    cudaFree(h->tl); cudaFree(h->ll); cudaFree(h->divv); cudaFree(h->death); cudaFree(h->connected);
+    cudaFree(h->labels); cudaFree(h->cell_type); cudaFree(h->field_buf);
+    cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->counters);
+    free_tallies(h->t);
+    free_population(h);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,150 @@
+// Internal interface between the host engine (engine.cu) and the kernel
+// files. Nothing here crosses the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace glz {
+
+constexpr int kMaxSpecies = 8;
+constexpr int kMaxTypes = 64;
+
+// Lattice geometry. A plane has d == 1, dim == 2, four colours; a volume has
+// dim == 3 and eight.
+struct Geometry {
+    int w, h, d, dim, ncol, sites;
+    int n_off;          // energy neighbourhood (lattice.rs:69-88)
+    int off[26][3];
+    int ring_n;         // connectivity ring (connectivity.rs:23-29), 0 when off
+    int ring[26][3];
+    uint32_t adjacency[26];
+    int nm;             // exact moment sums per cell: 5 in a plane, 9 in a volume
+};
+
+// Per-type tables in device memory, row-major [type][...], index 0 the medium.
+struct TypeTables {
+    const float *contact;       // n_types * n_types
+    const float *target_volume, *lambda_volume, *target_surface, *lambda_surface;
+    const double *target_length, *lambda_length, *division_volume, *death_rate;
+    const uint8_t *connected;
+    const float *chemotaxis, *secretion, *uptake;  // n_types * n_species
+};
+
+// The per-cell tallies a colour pass reads, in the rotation that gives every
+// pass a snapshot without an extra launch:
+//   the value at the start of pass p is B[p % 2] + D[(p + 2) % 3];
+//   pass p adds its changes into D[p % 3], and on the way writes
+//   B[(p + 1) % 2] = B[p % 2] + D[(p + 2) % 3] and clears D[(p + 1) % 3],
+//   none of which any thread of pass p reads.
+// `vol_surf` words hold (volume, surface); `mom` holds nm int64 sums per cell.
+struct Tallies {
+    int2 *vs_base[2];
+    long long *vs_delta[3];
+    long long *mom_base[2];
+    long long *mom_delta[3];
+    int *vol_by_colour;  // ncol per cell: only the current colour's entry changes in a pass
+    int *anchor;         // 4 per cell (x, y, z, unused): the integer origin of the moment sums
+};
+
+struct SweepLaunch {
+    Geometry g;
+    TypeTables t;
+    int n_types, n_species;
+    float temperature;
+    int colour;
+    int32_t step;
+    uint64_t key_pick, key_accept;  // stream_key(seed, step, colour, 0 / 1)
+    uint32_t *labels;
+    const uint8_t *cell_type;
+    // this pass's view of the tallies
+    const int2 *vs_base;
+    const long long *vs_prev;
+    unsigned long long *vs_cur;
+    int2 *vs_next_base;
+    long long *vs_clear;
+    const long long *mom_base;
+    const long long *mom_prev;
+    unsigned long long *mom_cur;
+    long long *mom_next_base;
+    long long *mom_clear;
+    int *vol_by_colour;
+    const int *anchor;
+    int n_labels;
+    int has_length, tracks, has_chemotaxis;
+    const float *fields[kMaxSpecies];
+    int use_tma;
+    const void *tensor_map;  // CUtensorMap in device-visible memory, or null
+    int *error_flag;
+};
+
+cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream);
+
+struct FieldLaunch {
+    Geometry g;
+    int n_species;
+    int round;
+    const float *in[kMaxSpecies];
+    float *out[kMaxSpecies];
+    float d[kMaxSpecies], decay[kMaxSpecies];
+    int active[kMaxSpecies], last[kMaxSpecies];
+    const uint32_t *labels;
+    const uint8_t *cell_type;
+    const float *secretion, *uptake;
+};
+
+cudaError_t launch_field_round(const FieldLaunch &a, cudaStream_t stream);
+
+// Recount every tally from the lattice into base slot `slot`, clearing every
+// delta word: volume, per-colour volume, surface, anchor (first site in scan
+// order) and the exact moment sums.
+struct RecountLaunch {
+    Geometry g;
+    const uint32_t *labels;
+    int n_labels;
+    int2 *vs_base;
+    long long *mom_base;
+    long long *vs_delta[3];
+    long long *mom_delta[3];
+    int *vol_by_colour;
+    int *anchor;
+    int tracks;
+    int *error_flag;  // set to 2 when a label is not below n_labels
+};
+
+cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream);
+
+// Fold the pending deltas into the base: B[s] += D[pd]; D[pd] = 0.
+cudaError_t launch_settle(int2 *vs_base, long long *vs_delta, long long *mom_base, long long *mom_delta, int nm,
+                          int n_labels, int tracks, cudaStream_t stream);
+
+// The medium's volume and unlike-bond surface, counted from the lattice
+// (the sweep keeps no tally for label 0).
+cudaError_t launch_medium_count(const Geometry &g, const uint32_t *labels, unsigned long long *out,
+                                cudaStream_t stream);
+
+struct PopulationLaunch {
+    Geometry g;
+    TypeTables t;
+    uint32_t *labels;
+    const uint8_t *cell_type_in;
+    uint8_t *cell_type_out;  // may alias cell_type_in
+    int n_labels;
+    int cap;
+    const int2 *vs_base;     // settled tallies
+    const long long *mom_base;
+    const int *anchor;
+    uint64_t key_death;      // stream_key(seed, step, kPopulationStream, 0)
+    // scratch, n_labels entries each
+    unsigned char *mode;
+    double *plan;            // 6 per cell: centroid, axis
+    int *moved;
+    uint32_t *daughter;
+    int *counters;           // [0] daughters issued, [1] events
+};
+
+cudaError_t launch_population_plan(const PopulationLaunch &a, cudaStream_t stream);
+cudaError_t launch_population_apply(const PopulationLaunch &a, cudaStream_t stream);
+
+}  // namespace glz

@@ -1,0 +1,172 @@
+"""``GpuSimulation``: a run kept on the B200, over the C ABI.
+
+The Python face of include/glazier_gpu.h, shaped like the reference's
+``glazier_cuda::GpuSimulation`` (glazier-cuda/src/lib.rs:748-1271): build
+from a start (``from_start``, the ``from_cpu`` of lib.rs:814), ``step``,
+and copy ``labels``, ``field``, ``volumes`` and ``surfaces`` back.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import GLZ_DRIVER, GLZ_INVALID, GLZ_ODD_LATTICE, GLZ_UNSUPPORTED, ptr
+
+
+class GpuError(ValueError):
+    """A refused or failed device call (``GpuError``, lib.rs:723-746); a
+    ``ValueError`` as glazier-py raises it (glazier-py/src/lib.rs:13-15)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+_NAMES = {GLZ_ODD_LATTICE: "odd lattice", GLZ_DRIVER: "driver", GLZ_UNSUPPORTED: "unsupported", GLZ_INVALID: "invalid"}
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        raise GpuError(rc, _lib.last_error())
+
+
+class GpuSimulation:
+    """One run on the device.
+
+    ``model`` is a ``glazier_b200.blueprint.Model``; ``labels`` holds one
+    uint32 per site (x fastest, 0 the medium) and ``cell_type`` one uint8 per
+    label; ``fields`` is None (every species starts at its ``initial``) or an
+    (n_species, sites) array.
+    """
+
+    def __init__(self, model, labels, cell_type, fields=None, device: int | None = None):
+        L = _lib.lib()
+        if device is not None:
+            check(L.glz_set_device(int(device)))
+        self._keep: list = []
+        m = _lib.model_struct(model, self._keep)
+        lab = np.ascontiguousarray(labels, dtype=np.uint32).reshape(-1)
+        ct = np.ascontiguousarray(cell_type, dtype=np.uint8).reshape(-1)
+        fl = None
+        if fields is not None:
+            fl = np.ascontiguousarray(fields, dtype=np.float64).reshape(-1)
+            if fl.size != len(model.species) * lab.size:
+                raise GpuError(GLZ_INVALID, f"fields hold {fl.size} values for {len(model.species)} species")
+        if lab.size != model.sites:
+            raise GpuError(GLZ_INVALID, f"the label field has {lab.size} sites for a lattice of {model.sites}")
+        h = C.c_void_p()
+        check(L.glz_gpu_create(C.byref(m), ptr(lab), ptr(ct), ct.size, ptr(fl) if fl is not None else None, None,
+                               C.byref(h)))
+        self._h = h
+        self.model = model
+        self.sites = model.sites
+        self.shape = (model.depth, model.height, model.width)
+
+    @classmethod
+    def from_start(cls, start, fields=None, device: int | None = None) -> "GpuSimulation":
+        return cls(start.model, start.labels, start.cell_type, fields, device)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().glz_gpu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def step(self, steps: int = 1) -> None:
+        """``GpuSimulation::step`` (lib.rs:1055): run and wait."""
+        check(_lib.lib().glz_gpu_step(self._h, int(steps)))
+
+    def step_profiled(self, steps: int = 1) -> tuple:
+        """Run like ``step`` and return the device milliseconds of the colour
+        sweeps, the field step, and division and death."""
+        ms = (C.c_double * 3)()
+        check(_lib.lib().glz_gpu_step_profiled(self._h, int(steps), ms))
+        return ms[0], ms[1], ms[2]
+
+    def set_labels(self, labels) -> None:
+        """Restart from a lattice: upload it and recount every tally."""
+        lab = np.ascontiguousarray(labels, dtype=np.uint32).reshape(-1)
+        check(_lib.lib().glz_gpu_set_labels(self._h, ptr(lab), lab.size))
+
+    def set_labels_from(self, address: int, sites: int) -> None:
+        """``set_labels`` from a raw host address (e.g. pinned memory)."""
+        check(_lib.lib().glz_gpu_set_labels(self._h, C.c_void_p(address), int(sites)))
+
+    def labels_to(self, address: int, sites: int) -> None:
+        """Copy the lattice to a raw host address (e.g. pinned memory)."""
+        check(_lib.lib().glz_gpu_labels(self._h, C.c_void_p(address), int(sites)))
+
+    @property
+    def mcs(self) -> int:
+        return int(_lib.lib().glz_gpu_mcs(self._h))
+
+    @property
+    def n_labels(self) -> int:
+        return int(_lib.lib().glz_gpu_n_labels(self._h))
+
+    def labels(self) -> np.ndarray:
+        out = np.empty(self.sites, dtype=np.uint32)
+        check(_lib.lib().glz_gpu_labels(self._h, ptr(out), out.size))
+        return out
+
+    def labels_into(self, out: np.ndarray) -> np.ndarray:
+        """Copy the lattice into a caller's buffer (pinned host memory works)."""
+        check(_lib.lib().glz_gpu_labels(self._h, ptr(out), out.size))
+        return out
+
+    def field(self, index: int) -> np.ndarray:
+        out = np.empty(self.sites, dtype=np.float64)
+        check(_lib.lib().glz_gpu_field(self._h, int(index), ptr(out), out.size))
+        return out
+
+    def _per_label(self, name: str, dtype) -> np.ndarray:
+        n = C.c_size_t(self.n_labels)
+        out = np.empty(n.value, dtype=dtype)
+        check(getattr(_lib.lib(), name)(self._h, ptr(out), C.byref(n)))
+        return out[: n.value]
+
+    def volumes(self) -> np.ndarray:
+        return self._per_label("glz_gpu_volumes", np.uint32)
+
+    def surfaces(self) -> np.ndarray:
+        return self._per_label("glz_gpu_surfaces", np.int64)
+
+    def cell_types(self) -> np.ndarray:
+        return self._per_label("glz_gpu_cell_types", np.uint8)
+
+    def set_nematic_field(self, pairs) -> None:
+        flat = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1)
+        check(_lib.lib().glz_gpu_set_nematic_field(self._h, ptr(flat), flat.size))
+
+    @property
+    def stream(self) -> int:
+        """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(_lib.lib().glz_gpu_stream(self._h) or 0)
+
+    def device_labels(self) -> int:
+        p = C.c_void_p()
+        check(_lib.lib().glz_gpu_device_labels(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def device_field(self, index: int) -> int:
+        p = C.c_void_p()
+        check(_lib.lib().glz_gpu_device_field(self._h, int(index), C.byref(p)))
+        return int(p.value or 0)

@@ -1,0 +1,155 @@
+/*
+ * glazier_gpu.h — the C ABI of the B200 Cellular Potts device engine.
+ *
+ * Every entry point replaces one item of the reference device backend,
+ * glazier-cuda/src/lib.rs (`GpuSimulation`, `GpuError`), and the glazier-py
+ * `GpuSession` built on it (glazier-py/src/lib.rs:184-241). The citations
+ * beside each declaration name the reference item it stands in for.
+ *
+ * Conventions
+ *   - Plain pointers and sizes; the caller owns every buffer it passes.
+ *   - Every call returns a status: GLZ_OK, or a code with a message that
+ *     glz_last_error() returns for the calling thread.
+ *   - One handle owns one CUDA stream on one device. A handle is not safe to
+ *     use from two threads at once (the reference `GpuSession` is
+ *     `unsendable`); distinct handles are independent.
+ *   - A model term the device engine does not run is refused at creation
+ *     with GLZ_UNSUPPORTED, never dropped silently (lib.rs:819-821).
+ */
+#ifndef GLAZIER_GPU_H
+#define GLAZIER_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. GpuError::OddLattice and GpuError::Driver (lib.rs:723-746)
+ * are GLZ_ODD_LATTICE and GLZ_DRIVER; the other two are refusals the
+ * reference raises as Driver strings or does not need. */
+enum {
+    GLZ_OK = 0,
+    GLZ_ODD_LATTICE = 1, /* message contains "even sides" (gpu_matches_cpu.rs:146) */
+    GLZ_DRIVER = 2,      /* a CUDA call failed */
+    GLZ_UNSUPPORTED = 3, /* a model term this engine does not run */
+    GLZ_INVALID = 4      /* a bad argument: null pointer, wrong length, bad index */
+};
+
+/*
+ * The model, as glazier-core/src/model.rs:9-76 states it, flattened.
+ * Per-type arrays hold n_types entries with index 0 the medium; the
+ * per-type-per-species tables are row-major [type][species]. Pointers the
+ * model does not need may be NULL (read as zeros). `nematic` is NULL or
+ * 2 * sites values (Q_xx, Q_xy) per site.
+ */
+typedef struct glz_model {
+    int32_t width, height, depth, neighbour_order;
+    int32_t n_types, n_species;
+    double temperature;
+    uint64_t seed;
+    const double *contact; /* n_types * n_types, symmetric */
+    const double *target_volume, *lambda_volume, *target_surface, *lambda_surface;
+    const double *division_volume, *death_rate, *target_length, *lambda_length;
+    const uint8_t *connected;
+    const double *max_activity, *lambda_activity, *external /* 3 per type */, *lambda_nematic;
+    const double *diffusion, *decay, *initial; /* n_species */
+    const double *secretion, *uptake, *chemotaxis; /* n_types * n_species */
+    const double *nematic;
+} glz_model;
+
+typedef struct glz_gpu glz_gpu;
+
+/* Make CUDA device `ordinal` current for this thread's later calls (the
+ * reference always takes device 0, lib.rs:823; one process per GPU picks its
+ * own). */
+int glz_set_device(int ordinal);
+
+/* The message of the last failed call on this thread (`GpuError` Display,
+ * lib.rs:730-740). Never NULL. */
+const char *glz_last_error(void);
+
+/*
+ * Upload a start and build the device state: GpuSimulation::from_cpu
+ * (lib.rs:814-1049).
+ *   labels     sites = width*height*depth labels, x fastest, 0 the medium
+ *   cell_type  n_labels types, index 0 the medium; n_labels > max label
+ *   fields     NULL (each species starts at its `initial`) or
+ *              n_species * sites concentrations, species-major
+ *   activity   NULL; a nonzero activity needs the motility term, refused
+ * Refuses odd sides (GLZ_ODD_LATTICE, lib.rs:816-818) and the nematic,
+ * motility and drift terms (GLZ_UNSUPPORTED).
+ */
+int glz_gpu_create(const glz_model *model, const uint32_t *labels, const uint8_t *cell_type, size_t n_labels,
+                   const double *fields, const double *activity, glz_gpu **out);
+
+/* Run `steps` Monte Carlo steps and wait for them: GpuSimulation::step
+ * (lib.rs:1055-1144). */
+int glz_gpu_step(glz_gpu *h, uint64_t steps);
+
+/* Replace the lattice and recount every tally from it, keeping the cell
+ * types, fields and step count: a restart from a label field
+ * (Simulation::from_labels, glazier-core/src/cpu.rs:151-175, as the
+ * Blueprint's `initial.labels` uses it). Labels are checked on the device;
+ * one not below the label count fails the next glz_gpu_step. */
+int glz_gpu_set_labels(glz_gpu *h, const uint32_t *labels, size_t sites);
+
+/* Run `steps` Monte Carlo steps like glz_gpu_step and report the device time
+ * of each phase in milliseconds: ms[0] the colour sweeps, ms[1] the field
+ * step, ms[2] division and death. No reference counterpart. */
+int glz_gpu_step_profiled(glz_gpu *h, uint64_t steps, double ms[3]);
+
+/* Copy the lattice back, `sites` labels: GpuSimulation::labels (lib.rs:1227). */
+int glz_gpu_labels(glz_gpu *h, uint32_t *out, size_t sites);
+
+/* Copy species `index` back as f64, `sites` values: GpuSimulation::field
+ * (lib.rs:1235-1242). */
+int glz_gpu_field(glz_gpu *h, int index, double *out, size_t sites);
+
+/* Per-label volumes, index 0 the medium, clamped at zero:
+ * GpuSimulation::volumes (lib.rs:1262-1270). `*count` holds the capacity of
+ * `out` on entry and the label count on return; a short buffer is
+ * GLZ_INVALID with the needed count in `*count`. */
+int glz_gpu_volumes(glz_gpu *h, uint32_t *out, size_t *count);
+
+/* Per-label unlike-bond surfaces: GpuSimulation::surfaces (lib.rs:1248-1256).
+ * `*count` as for glz_gpu_volumes. */
+int glz_gpu_surfaces(glz_gpu *h, int64_t *out, size_t *count);
+
+/* Per-label cell types (the host mirror `cell_type_host`, lib.rs:799).
+ * `*count` as for glz_gpu_volumes. */
+int glz_gpu_cell_types(glz_gpu *h, uint8_t *out, size_t *count);
+
+/* Replace the nematic field, 2 * sites values: GpuSimulation::set_nematic_field
+ * (lib.rs:1199-1221). A model without a nematic coupling is refused with the
+ * reference's message. */
+int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len);
+
+/* Monte Carlo steps completed: `pub mcs` (lib.rs:805). */
+uint64_t glz_gpu_mcs(const glz_gpu *h);
+
+/* Labels ever issued, the medium included (`cell_type_host.len()`,
+ * lib.rs:1365). */
+size_t glz_gpu_n_labels(const glz_gpu *h);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against the engine's. No reference counterpart: the
+ * reference keeps its stream private (lib.rs:751). */
+void *glz_gpu_stream(glz_gpu *h);
+
+/* Device addresses of the lattice (uint32 per site) and of species `index`
+ * (f32 per site), valid until the next glz_gpu_step or glz_gpu_destroy; for
+ * a caller that couples another solver on the device (the zero-copy form of
+ * GpuSession.labels, glazier-py/src/lib.rs:215-219). */
+int glz_gpu_device_labels(glz_gpu *h, void **labels);
+int glz_gpu_device_field(glz_gpu *h, int index, void **field);
+
+/* Release the device state: Drop for GpuSimulation. NULL is a no-op. */
+void glz_gpu_destroy(glz_gpu *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GLAZIER_GPU_H */

@@ -1,0 +1,70 @@
+"""The ``_native`` entry points on the device engine.
+
+Restates glazier's tests/test_native_engine.py (the run shape and the
+volume sum) and drives ``GpuSession`` the way glazier-py exposes it.
+"""
+
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from glazier_b200 import native
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "serial_reference.json").read_text())
+MONOLAYER = GOLDEN["parse"]["monolayer.json"]["text"]
+
+
+def test_a_short_run_returns_a_lattice_of_the_stated_shape(device):
+    # tests/test_native_engine.py:27-37
+    labels, width, height, depth = native.run(MONOLAYER, 5)
+    field = np.asarray(labels, dtype=np.uint32).reshape(depth, height, width)
+    parsed = native.parse(MONOLAYER)
+    assert field.shape == (parsed["depth"], parsed["height"], parsed["width"])
+    side, nx, ny, nz = parsed["initial"]
+    assert np.unique(field[field > 0]).size == nx * ny * nz
+
+
+def test_volumes_come_back_per_cell(device):
+    # tests/test_native_engine.py:40-48
+    volumes = native.run_volumes(MONOLAYER, 5)
+    parsed = native.parse(MONOLAYER)
+    side, nx, ny, nz = parsed["initial"]
+    assert len(volumes) == nx * ny * nz + 1
+    assert sum(volumes[1:]) == parsed["width"] * parsed["height"] * parsed["depth"]
+
+
+def test_a_session_keeps_the_run_on_the_device(device):
+    # glazier-py/src/lib.rs:184-241
+    session = native.GpuSession(MONOLAYER)
+    assert session.mcs == 0
+    session.step(3)
+    session.step(2)
+    assert session.mcs == 5
+    labels = session.labels()
+    assert len(labels) == 128 * 128
+    with pytest.raises(ValueError, match="expected"):
+        session.set_nematic_field([0.0, 0.0])
+    with pytest.raises(ValueError, match="no nematic coupling"):
+        session.set_nematic_field([0.0] * (2 * 128 * 128))
+
+
+def test_every_reference_blueprint_the_engine_runs_starts_and_steps(device):
+    ran = 0
+    for name, entry in GOLDEN["parse"].items():
+        raw = json.loads(entry["text"])
+        if raw.get("nematic_field") or raw["initial"].get("labels"):
+            continue
+        if any(t.get("max_activity", 0) or any(t.get("external", [0, 0, 0])) for t in raw["types"]):
+            with pytest.raises(ValueError):
+                native.GpuSession(entry["text"])
+            continue
+        session = native.GpuSession(entry["text"])
+        session.step(2)
+        ran += 1
+    assert ran >= 8

@@ -1,0 +1,143 @@
+"""Bit-exact parity: the device engine against the host replay of its schedule.
+
+Every case runs the same start on the B200 (through the C ABI) and on the
+replay (oracle/replay.c) and requires identical labels, per-label volumes,
+surfaces and cell types, and bit-identical f32 fields. Each case runs with
+the sweep's tensor-copy window load on and off, so both load paths are held
+to the same result.
+"""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import sheet_model, tiled, with_species
+from glazier_b200.blueprint import Start
+from oracle.replay import ReplayOracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _plain():
+    return tiled(sheet_model(seed=1)), 20
+
+
+def _surface():
+    return tiled(sheet_model(seed=3, target_surface=34.0, lambda_surface=0.1)), 20
+
+
+def _von_neumann():
+    return tiled(sheet_model(seed=5, order=1, contact=(0, 12, 12, 6))), 20
+
+
+def _large():
+    m = sheet_model(width=256, height=192, seed=2, contact=(0, 10, 10, 10), lambda_volume=1.0,
+                    target_surface=92.0, lambda_surface=0.2)
+    return tiled(m), 10
+
+
+def _unaligned():
+    # 34 columns: rows are not whole 16-byte units, so the window takes plain loads
+    return tiled(sheet_model(width=34, height=22, seed=4), 6), 25
+
+
+def _medium():
+    m = sheet_model(width=96, height=64, seed=6)
+    return tiled(m, 8, 6, 4), 20
+
+
+def _volume(order):
+    def make():
+        m = sheet_model(width=32, height=32, depth=32, seed=31, target_volume=512.0, order=order,
+                        target_surface=3176.0 if order == 3 else 0.0, lambda_surface=0.2 if order == 3 else 0.0)
+        return tiled(m), 6
+    return make
+
+
+def _volume_wide():
+    m = sheet_model(width=96, height=32, depth=32, seed=8, target_volume=512.0, order=3, contact=(0, 10, 10, 10),
+                    lambda_volume=1.0)
+    return tiled(m), 4
+
+
+def _fields():
+    m = with_species(sheet_model(seed=11), [("IFNg", 0.4, 0.01, 0.0), ("b", 0.7, 0.02, 1.0)],
+                     [[0.0, 0.0], [0.2, 0.0]], [[0.0, 0.0], [0.01, 0.1]], [[0.0, 0.0], [3.0, -2.0]])
+    return tiled(m), 20
+
+
+def _length():
+    return tiled(sheet_model(seed=41, target_length=24.0, lambda_length=1.0)), 20
+
+
+def _length_volume():
+    m = sheet_model(width=32, height=32, depth=32, seed=12, target_volume=512.0, order=3,
+                    target_length=14.0, lambda_length=0.5)
+    return tiled(m), 3
+
+
+def _connected():
+    m = sheet_model(seed=23, contact=(0, 4, 4, 4), lambda_volume=1.0, temperature=40.0, connected=True)
+    return tiled(m), 20
+
+
+def _population():
+    m = sheet_model(seed=8, division_volume=72.0, death_rate=0.005, target_volume=100.0)
+    return tiled(m, 6, 6, 6), 40
+
+
+def _chemotaxis_ramp():
+    m = with_species(sheet_model(seed=21), [("attractant", 0.0, 0.0, 0.0)], [[0.0], [0.0]], [[0.0], [0.0]],
+                     [[0.0], [4.0]])
+    labels = np.zeros(64 * 64, dtype=np.uint32)
+    ys, xs = np.divmod(np.arange(64 * 64), 64)
+    labels[(xs >= 24) & (xs < 32) & (ys >= 24) & (ys < 32)] = 1
+    start = Start(m, labels, np.array([0, 1], dtype=np.uint8))
+    fields = xs.astype(np.float64)[None, :]
+    return (start, fields), 30
+
+
+CASES = {
+    "plain": _plain,
+    "surface": _surface,
+    "von-neumann": _von_neumann,
+    "large": _large,
+    "unaligned": _unaligned,
+    "medium": _medium,
+    "volume-26": _volume(3),
+    "volume-18": _volume(2),
+    "volume-6": _volume(1),
+    "volume-wide": _volume_wide,
+    "fields": _fields,
+    "length": _length,
+    "length-volume": _length_volume,
+    "connected": _connected,
+    "population": _population,
+    "chemotaxis-ramp": _chemotaxis_ramp,
+}
+
+
+@pytest.mark.parametrize("tma", ["1", "0"])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, monkeypatch):
+    made, steps = CASES[name]()
+    start, fields = made if isinstance(made, tuple) else (made, None)
+    monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
+    gpu = device.GpuSimulation.from_start(start, fields)
+    replay = ReplayOracle.from_start(start, fields)
+    for chunk in (1, steps - 1):
+        gpu.step(chunk)
+        replay.step(chunk)
+        assert gpu.n_labels == replay.n_labels
+        labels = gpu.labels()
+        want = replay.labels()
+        assert np.array_equal(labels, want), f"{int((labels != want).sum())} sites differ after {gpu.mcs} MCS"
+        assert np.array_equal(gpu.volumes(), replay.volumes())
+        assert np.array_equal(gpu.surfaces(), replay.surfaces())
+        assert np.array_equal(gpu.cell_types(), replay.cell_types())
+        for k in range(len(start.model.species)):
+            assert np.array_equal(gpu.field(k).astype(np.float32), replay.field(k))
+    gpu.close()

@@ -1,0 +1,218 @@
+"""The reference's own device tests, run on the B200 engine.
+
+Each test restates one of glazier-tests' GPU tests (file:line given) with the
+same model, the same steps and the same band, the serial oracle standing in
+for the reference's serial engine.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import pieces, recount_volumes, sheet_model, spread, tiled, with_species
+from glazier_b200.blueprint import Start
+from oracle.serial import SerialOracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _serial(model, steps, start=None):
+    o = SerialOracle.from_start(start or tiled(model))
+    o.step(steps)
+    return o
+
+
+def test_the_gpu_reproduces_the_serial_run_in_distribution(device):
+    # gpu_matches_cpu.rs:48-92
+    m = sheet_model(seed=1)
+    cpu = _serial(m, 200)
+    gpu = device.GpuSimulation.from_start(tiled(m))
+    gpu.step(200)
+    vc, vg = cpu.volumes()[1:], gpu.volumes()
+    assert vc.size == vg.size - 1, "cell counts differ"
+    assert abs(vc.mean() - vg[1:].mean()) < 1e-9
+    sc, sg = spread(vc, 64.0), spread(vg[1:], 64.0)
+    assert abs(sc - sg) / max(sc, sg) < 0.25, (sc, sg)
+    assert np.array_equal(recount_volumes(gpu.labels(), gpu.n_labels), vg), "the device volume counter drifted"
+
+
+def test_the_device_surface_counter_matches_the_lattice_it_wrote(device):
+    # gpu_matches_cpu.rs:103-118
+    m = sheet_model(seed=3, target_surface=34.0, lambda_surface=0.1)
+    gpu = device.GpuSimulation.from_start(tiled(m))
+    gpu.step(150)
+    check = SerialOracle(m, labels=gpu.labels(), cell_type=gpu.cell_types())
+    assert np.array_equal(gpu.surfaces(), check.recounted_surfaces())
+
+
+def test_a_device_run_conserves_its_cells(device):
+    # gpu_matches_cpu.rs:120-138
+    gpu = device.GpuSimulation.from_start(tiled(sheet_model(seed=7)))
+    gpu.step(300)
+    v = gpu.volumes()
+    assert v.size - 1 == 64 and (v[1:] >= 1).all()
+
+
+def test_the_device_refuses_a_lattice_it_cannot_colour(device):
+    # gpu_matches_cpu.rs:140-149
+    m = sheet_model(width=33, height=32)
+    start = Start.tiled(m, 8)
+    with pytest.raises(device.GpuError, match="even sides"):
+        device.GpuSimulation.from_start(start)
+
+
+def test_the_device_stretches_cells_the_way_the_serial_engine_does(device):
+    # gpu_matches_cpu.rs:155-203
+    stated = sheet_model(seed=41, target_length=24.0, lambda_length=1.0)
+    cpu = _serial(stated, 200)
+    gpu = device.GpuSimulation.from_start(tiled(stated))
+    gpu.step(200)
+    on_device = SerialOracle(stated, labels=gpu.labels(), cell_type=gpu.cell_types())
+    free = _serial(sheet_model(seed=41), 200).lengths()[1:].mean()
+    serial = cpu.lengths()[1:].mean()
+    dev = on_device.lengths()[1:].mean()
+    assert serial > free and dev > free
+    assert abs(serial - dev) / max(serial, dev) < 0.15, (serial, dev)
+
+
+def _secreting(seed):
+    return with_species(sheet_model(seed=seed), [("IFNg", 0.4, 0.01, 0.0)], [[0.0], [0.2]], [[0.0], [0.01]],
+                        [[0.0], [0.0]])
+
+
+def test_the_device_solves_a_field_the_way_the_serial_engine_does(device):
+    # gpu_matches_cpu.rs:230-257
+    cpu = _serial(_secreting(11), 60)
+    gpu = device.GpuSimulation.from_start(tiled(_secreting(11)))
+    gpu.step(60)
+    dev, ser = gpu.field(0).sum(), cpu.field(0).sum()
+    assert dev > 0
+    assert abs(dev - ser) / max(dev, ser) < 0.02
+
+
+def test_a_device_field_stays_where_it_started_without_sources(device):
+    # gpu_matches_cpu.rs:259-285
+    m = _secreting(12)
+    m.secretion = [[0.0], [0.0]]
+    m.uptake = [[0.0], [0.0]]
+    m.species[0].decay = 0.0
+    m.species[0].initial = 2.0
+    gpu = device.GpuSimulation.from_start(tiled(m))
+    gpu.step(40)
+    total = gpu.field(0).sum()
+    assert abs(total - 2.0 * 4096) / (2.0 * 4096) < 1e-4
+
+
+def test_the_device_climbs_a_gradient(device):
+    # gpu_matches_cpu.rs:287-336
+    m = with_species(sheet_model(seed=21), [("attractant", 0.0, 0.0, 0.0)], [[0.0], [0.0]], [[0.0], [0.0]],
+                     [[0.0], [4.0]])
+    ys, xs = np.divmod(np.arange(64 * 64), 64)
+    labels = ((xs >= 24) & (xs < 32) & (ys >= 24) & (ys < 32)).astype(np.uint32)
+    start = Start(m, labels, np.array([0, 1], dtype=np.uint8))
+    centre = lambda lab: xs[lab == 1].mean()  # noqa: E731
+    gpu = device.GpuSimulation.from_start(start, xs.astype(np.float64)[None, :])
+    gpu.step(300)
+    assert centre(gpu.labels()) - centre(labels) > 3.0
+
+
+def test_the_device_runs_a_volume(device):
+    # gpu_matches_cpu.rs:338-392
+    m = sheet_model(width=32, height=32, depth=32, seed=31, target_volume=512.0)
+    cpu = _serial(m, 40)
+    gpu = device.GpuSimulation.from_start(tiled(m))
+    gpu.step(40)
+    dv = gpu.volumes()
+    assert dv.size == cpu.n_labels
+    assert int(dv[1:].sum()) == int(cpu.volumes()[1:].sum())
+    assert np.array_equal(dv[1:], recount_volumes(gpu.labels(), dv.size)[1:])
+    sc, sg = spread(cpu.volumes()[1:], 512.0), spread(dv[1:], 512.0)
+    assert abs(sc - sg) / max(sc, sg) < 0.3, (sc, sg)
+
+
+def _pop_model(division_volume, death_rate, target_volume, seed):
+    return sheet_model(seed=seed, division_volume=division_volume, death_rate=death_rate, target_volume=target_volume)
+
+
+def _live(v):
+    return int((np.asarray(v)[1:] > 0).sum())
+
+
+def test_the_device_kills_cells_at_the_stated_rate(device):
+    # gpu_population.rs:45-59
+    start = tiled(_pop_model(0.0, 0.02, 64.0, 5), 8, 6, 6)
+    gpu = device.GpuSimulation.from_start(start)
+    gpu.step(50)
+    expected = start.n_cells * 0.98**50
+    assert abs(_live(gpu.volumes()) - expected) < 0.35 * start.n_cells
+
+
+def test_a_dead_cell_leaves_medium_on_the_device(device):
+    # gpu_population.rs:61-78
+    gpu = device.GpuSimulation.from_start(tiled(_pop_model(0.0, 1.0, 64.0, 6), 8, 2, 2))
+    gpu.step(1)
+    assert _live(gpu.volumes()) == 0
+    assert (gpu.labels() == 0).all()
+
+
+def test_the_device_divides_and_conserves_the_sites(device):
+    # gpu_population.rs:80-99
+    start = tiled(_pop_model(40.0, 0.0, 100.0, 7), 8, 4, 4)
+    gpu = device.GpuSimulation.from_start(start)
+    gpu.step(1)
+    v = gpu.volumes()
+    assert _live(v) > start.n_cells
+    assert int(v[1:].sum()) == int((gpu.labels() != 0).sum())
+
+
+def test_the_device_counters_match_the_lattice_they_wrote(device):
+    # gpu_population.rs:101-117
+    gpu = device.GpuSimulation.from_start(tiled(_pop_model(72.0, 0.005, 100.0, 8), 6, 6, 6))
+    gpu.step(120)
+    v = gpu.volumes()
+    assert np.array_equal(v[1:], recount_volumes(gpu.labels(), v.size)[1:])
+
+
+def test_both_engines_lose_cells_at_the_rate_the_description_states(device):
+    # gpu_population.rs:119-153
+    steps, rate = 80, 0.01
+    start = tiled(_pop_model(0.0, rate, 64.0, 9), 8, 10, 10)
+    cpu = SerialOracle.from_start(start)
+    cpu.step(steps)
+    gpu = device.GpuSimulation.from_start(start)
+    gpu.step(steps)
+    survival = (1 - rate) ** steps
+    expected = start.n_cells * survival
+    sd = math.sqrt(start.n_cells * survival * (1 - survival))
+    for name, left in (("serial", _live(cpu.volumes())), ("device", _live(gpu.volumes()))):
+        assert abs(left - expected) < 3 * sd, (name, left, expected, sd)
+
+
+def _conn_model(connected, temperature):
+    return sheet_model(seed=23, contact=(0, 4, 4, 4), lambda_volume=1.0, temperature=temperature,
+                       connected=connected)
+
+
+def test_the_device_keeps_cells_whole_where_nothing_else_does(device):
+    # glazier-tests/tests/connectivity.rs:120-155
+    loose = device.GpuSimulation.from_start(tiled(_conn_model(False, 40.0)))
+    whole = device.GpuSimulation.from_start(tiled(_conn_model(True, 40.0)))
+    loose.step(200)
+    whole.step(200)
+    assert pieces(loose.labels(), 64, 64) > 64
+    assert pieces(whole.labels(), 64, 64) == 64
+
+
+def test_the_device_and_the_serial_engine_agree_on_a_constrained_sheet(device):
+    # glazier-tests/tests/connectivity.rs:157-189
+    m = _conn_model(True, 20.0)
+    cpu = _serial(m, 150)
+    gpu = device.GpuSimulation.from_start(tiled(m))
+    gpu.step(150)
+    dv = gpu.volumes()
+    assert int(dv[1:].sum()) == int(cpu.volumes()[1:].sum())
+    sc, sg = spread(cpu.volumes()[1:], 64.0), spread(dv[1:], 64.0)
+    assert abs(sc - sg) / max(sc, sg) < 0.3, (sc, sg)
