@@ -101,7 +101,7 @@ struct glz_gpu {
     cudaStream_t stream = nullptr;
     glz::Geometry g{};
     int n_types = 0, n_species = 0;
-    float temperature = 0.0f;
+    float beta = 0.0f;
     uint64_t seed = 0;
     bool has_length = false, tracks = false, has_chemotaxis = false, has_pop = false;
     int substeps[glz::kMaxSpecies] = {};
@@ -123,6 +123,7 @@ struct glz_gpu {
     int field_cur[glz::kMaxSpecies] = {};
     uint64_t pass_no = 0, mcs = 0;
     bool use_tma = false;
+    int max_ctas = 0;
     CUtensorMap tmap{};
     int *error_flag = nullptr;
     unsigned long long *medium = nullptr;
@@ -279,7 +280,7 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.t = h->tables();
     a.n_types = h->n_types;
     a.n_species = h->n_species;
-    a.temperature = h->temperature;
+    a.beta = h->beta;
     a.colour = colour;
     a.step = (int32_t)h->mcs;
     a.key_pick = glz::stream_key(h->seed, a.step, colour, 0);
@@ -304,6 +305,7 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.has_chemotaxis = h->has_chemotaxis;
     for (int s = 0; s < h->n_species; ++s) a.fields[s] = h->field_ptr(s, h->field_cur[s]);
     a.use_tma = h->use_tma;
+    a.max_ctas = h->max_ctas;
     a.tensor_map = h->use_tma ? &h->tmap : nullptr;
     a.error_flag = h->error_flag;
     CU(glz::launch_sweep(a, h->stream));
@@ -390,6 +392,7 @@ int check_error_flag(glz_gpu *h) {
     CU(cudaStreamSynchronize(h->stream));
     if (flag == 1) return fail(GLZ_DRIVER, "a sweep tile's tensor copy did not complete within its wait limit");
     if (flag == 2) return fail(GLZ_INVALID, "a label is not below the cell type count");
+    if (flag == 3) return fail(GLZ_DRIVER, "the sweep's shared-memory window was not 128-byte aligned");
     return GLZ_OK;
 }
 
@@ -495,7 +498,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     g.n_off = offsets_for(m->neighbour_order, d, g.off);
     h->n_types = nt;
     h->n_species = ns;
-    h->temperature = (float)m->temperature;
+    h->beta = (float)(1.0 / m->temperature);
     h->seed = m->seed;
 
     std::vector<float> contact(nt * nt), tv(nt), lv(nt), ts(nt), ls(nt);
@@ -577,6 +580,9 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     // The tensor copy needs rows that are a whole number of 16-byte units.
     const char *env = std::getenv("GLAZIER_SWEEP_TMA");
     h->use_tma = (w % 4 == 0) && !(env && env[0] == '0');
+    // GLAZIER_SWEEP_CTAS caps the sweep's persistent grid; the default is one
+    // full wave of resident CTAs.
+    if (const char *cap = std::getenv("GLAZIER_SWEEP_CTAS")) h->max_ctas = std::atoi(cap);
     if (h->use_tma) {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q;

@@ -52,7 +52,7 @@ struct SweepLaunch {
     Geometry g;
     TypeTables t;
     int n_types, n_species;
-    float temperature;
+    float beta;  // (float)(1 / T), rounded once on the host
     int colour;
     int32_t step;
     uint64_t key_pick, key_accept;  // stream_key(seed, step, colour, 0 / 1)
@@ -75,6 +75,7 @@ struct SweepLaunch {
     int has_length, tracks, has_chemotaxis;
     const float *fields[kMaxSpecies];
     int use_tma;
+    int max_ctas;            // > 0 caps the persistent grid (each CTA then walks more tiles)
     const void *tensor_map;  // CUtensorMap in device-visible memory, or null
     int *error_flag;
 };

@@ -1,15 +1,25 @@
 // The checkerboard Metropolis copy sweep: one launch per colour.
 //
 // Replaces `cpm_sweep` of the reference device engine (glazier-cuda/src/
-// lib.rs:436-716). Each CTA owns a tile of the lattice, stages the tile and a
-// one-site halo of labels in shared memory (a TMA tensor copy for tiles away
-// from the periodic edge, wrapped plain loads elsewhere), and prices every
-// target of the pass's colour in it. Same-colour targets are two apart on
-// every axis, outside any neighbourhood, so a pass's copies are independent
-// and the labels a target reads do not change during the pass.
+// lib.rs:436-716). Same-colour targets are two apart on every axis, outside
+// any neighbourhood, so a pass's copies are independent and the labels a
+// target reads do not change during the pass.
+//
+// Layout of the work:
+//   - Persistent CTAs walk the lattice tile by tile. A tile and its one-site
+//     halo are staged in shared memory; tiles clear of the periodic edge
+//     arrive by a TMA tensor copy issued one tile ahead into the other of two
+//     buffers, so the copy of tile i+1 overlaps the work on tile i. Edge
+//     tiles, and lattices whose rows are not whole 16-byte units, take
+//     wrapped plain loads.
+//   - Each warp first draws every target's neighbour pick (one counter-hash
+//     draw per target) and keeps only the targets whose neighbour carries
+//     another label, about a fifth of them in a tissue, in a per-warp queue;
+//     it then prices the queued copies densely, one per lane. The expensive
+//     path never runs with idle lanes that a light target left behind.
 //
 // Per-cell tallies (volume, surface, exact moment sums) are read from the
-// snapshot the rotation in engine.h gives each pass, and changed by integer
+// snapshot the rotation in engine.h gives each pass and changed by integer
 // atomics whose order does not matter; a pass is therefore deterministic and
 // a host replay of the same schedule reproduces it bit for bit.
 
@@ -25,7 +35,7 @@ struct Tile;
 
 template <>
 struct Tile<2> {
-    static constexpr int TX = 64, TY = 32, TZ = 1;
+    static constexpr int TX = 128, TY = 32, TZ = 1;
     static constexpr int HX = 4;  // x halo rounded up to 16 bytes for the tensor copy
     static constexpr int PX = TX + 2 * HX, PY = TY + 2, PZ = 1;
     static constexpr int HZ = 0;
@@ -34,16 +44,32 @@ struct Tile<2> {
 
 template <>
 struct Tile<3> {
-    static constexpr int TX = 32, TY = 8, TZ = 8;
+    static constexpr int TX = 64, TY = 8, TZ = 8;
     static constexpr int HX = 4;
     static constexpr int PX = TX + 2 * HX, PY = TY + 2, PZ = TZ + 2;
     static constexpr int HZ = 1;
     static constexpr int NT = (TX / 2) * (TY / 2) * (TZ / 2);
 };
 
-constexpr int kSweepThreads = 256;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 constexpr int kSmemTypes = 16;  // contact tables up to 16 types live in shared memory
-constexpr long long kWaitLimit = 1LL << 22;
+constexpr long long kWaitLimit = 1LL << 24;
+
+template <int DIM>
+struct SweepSmem {
+    static constexpr int WIN = Tile<DIM>::PX * Tile<DIM>::PY * Tile<DIM>::PZ;
+    // A tensor copy's shared-memory destination must sit on a 128-byte
+    // boundary, so each window buffer is padded to a multiple of 32 labels.
+    static constexpr int WIN_STRIDE = (WIN + 31) / 32 * 32;
+    static constexpr int TPW = Tile<DIM>::NT / kWarps;  // targets per warp per tile
+    alignas(128) uint32_t win[2][WIN_STRIDE];
+    uint32_t queue[kWarps][TPW];
+    float contact[kSmemTypes * kSmemTypes];
+    int woff[26];
+    int wring[26];
+    alignas(8) unsigned long long mbar[2];
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -112,8 +138,8 @@ __device__ __forceinline__ void site_terms(int ux, int uy, int uz, long long *t)
 // Change in a cell's length energy (cpu.rs:291-305) when the site with sum
 // terms `terms` leaves (sign -1) or joins (+1) it, from the pass snapshot.
 template <int DIM>
-__device__ double length_delta(const SweepLaunch &a, int type, int label, long long n, const long long *terms,
-                               int sign) {
+__device__ __noinline__ double length_delta(const SweepLaunch &a, int type, int label, long long n,
+                                            const long long *terms, int sign) {
     constexpr int NM = DIM == 2 ? 5 : 9;
     long long m[NM], after[NM];
 #pragma unroll
@@ -145,18 +171,259 @@ __device__ __forceinline__ bool one_piece(uint32_t present, const uint32_t *adja
     return reached == present;
 }
 
+// Position of target j of a tile: local coordinates in the tile.
+template <int DIM>
+__device__ __forceinline__ void target_of(int j, int colour, int &lx, int &ly, int &lz) {
+    using T = Tile<DIM>;
+    const int jx = j % (T::TX / 2);
+    const int jy = (j / (T::TX / 2)) % (T::TY / 2);
+    const int jz = DIM == 3 ? j / ((T::TX / 2) * (T::TY / 2)) : 0;
+    lx = 2 * jx + (colour & 1);
+    ly = 2 * jy + ((colour >> 1) & 1);
+    lz = DIM == 3 ? 2 * jz + ((colour >> 2) & 1) : 0;
+}
+
+// Price one copy attempt whose neighbour pick is known to carry another label
+// and commit it if the Metropolis test takes it.
 template <int DIM, int NOFF>
-__global__ void __launch_bounds__(kSweepThreads) sweep_kernel(const __grid_constant__ SweepLaunch a,
-                                                              const __grid_constant__ CUtensorMap tmap) {
+__device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const SweepSmem<DIM> &S, const uint32_t *win,
+                                                 uint32_t entry, int x0, int y0, int z0, bool small_types) {
     using T = Tile<DIM>;
     constexpr int NM = DIM == 2 ? 5 : 9;
-    __shared__ alignas(128) uint32_t win[T::PX * T::PY * T::PZ];
-    __shared__ float s_contact[kSmemTypes * kSmemTypes];
-    __shared__ alignas(8) unsigned long long mbar;
-    __shared__ int s_woff[26];
-    __shared__ int s_wring[26];
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    const int j = (int)(entry & 0xffffu);
+    const int pick = (int)(entry >> 16);
+    int lx, ly, lz;
+    target_of<DIM>(j, a.colour, lx, ly, lz);
+    const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+    const uint32_t target = (uint32_t)(((size_t)z * H + y) * W + x);
+    const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
+    const uint32_t old = win[wc];
+    const uint32_t nw = win[wc + S.woff[pick]];
 
-    const int tid = threadIdx.x;
+    // The snapshot tallies of both cells, requested before the neighbour loop
+    // so their latency hides behind it.
+    long long prev_old = 0, prev_new = 0;
+    int2 base_old = make_int2(0, 0), base_new = make_int2(0, 0);
+    if (old != 0) {
+        base_old = a.vs_base[old];
+        prev_old = a.vs_prev[old];
+    }
+    if (nw != 0) {
+        base_new = a.vs_base[nw];
+        prev_new = a.vs_prev[nw];
+    }
+    const int t_old = a.cell_type[old], t_new = a.cell_type[nw];
+
+    float delta = 0.0f;
+    int like_old = 0, like_new = 0;
+#pragma unroll
+    for (int k = 0; k < NOFF; ++k) {
+        const uint32_t ln = win[wc + S.woff[k]];
+        const int tn = ln == old ? t_old : (ln == nw ? t_new : (int)a.cell_type[ln]);
+        if (ln != old) {
+            const float j_old = small_types ? S.contact[t_old * a.n_types + tn] : a.t.contact[t_old * a.n_types + tn];
+            delta = __fsub_rn(delta, j_old);
+        } else {
+            ++like_old;
+        }
+        if (ln != nw) {
+            const float j_new = small_types ? S.contact[t_new * a.n_types + tn] : a.t.contact[t_new * a.n_types + tn];
+            delta = __fadd_rn(delta, j_new);
+        } else {
+            ++like_new;
+        }
+    }
+
+    if (old != 0) {
+        // The per-colour guard: the losing cell must keep a site of another
+        // colour. A like neighbour is one, since every neighbour of a target
+        // is of another colour.
+        if (like_old == 0) {
+            int other = 0;
+            for (int c = 0; c < a.g.ncol; ++c)
+                if (c != a.colour) other += a.vol_by_colour[(size_t)old * a.g.ncol + c];
+            if (other == 0) return;
+        }
+        if (a.g.ring_n > 0 && a.t.connected[t_old]) {
+            uint32_t present = 0;
+            for (int k = 0; k < a.g.ring_n; ++k)
+                if (win[wc + S.wring[k]] == old) present |= 1u << k;
+            if (!one_piece(present, a.g.adjacency)) return;
+        }
+    }
+    const int ds_old = 2 * like_old - NOFF;
+    const int ds_new = NOFF - 2 * like_new;
+
+    int vol_old = 0, surf_old = 0, vol_new = 0, surf_new = 0;
+    {
+        int dv, ds;
+        unpack_delta(prev_old, dv, ds);
+        vol_old = base_old.x + dv;
+        surf_old = base_old.y + ds;
+        unpack_delta(prev_new, dv, ds);
+        vol_new = base_new.x + dv;
+        surf_new = base_new.y + ds;
+    }
+    // lambda ((v -/+ 1 - V_t)^2 - (v - V_t)^2) = lambda (1 -/+ 2 (v - V_t))
+    if (old != 0) {
+        const float lam = a.t.lambda_volume[t_old];
+        if (lam != 0.0f) {
+            const float dv = __fsub_rn((float)vol_old, a.t.target_volume[t_old]);
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, dv))));
+        }
+    }
+    if (nw != 0) {
+        const float lam = a.t.lambda_volume[t_new];
+        if (lam != 0.0f) {
+            const float dv = __fsub_rn((float)vol_new, a.t.target_volume[t_new]);
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fadd_rn(__fmul_rn(2.0f, dv), 1.0f)));
+        }
+    }
+    // lambda ((s + ds - S_t)^2 - (s - S_t)^2) = lambda ds (2 (s - S_t) + ds)
+    if (old != 0) {
+        const float lam = a.t.lambda_surface[t_old];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)surf_old, a.t.target_surface[t_old]), dsf = (float)ds_old;
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
+        }
+    }
+    if (nw != 0) {
+        const float lam = a.t.lambda_surface[t_new];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)surf_new, a.t.target_surface[t_new]), dsf = (float)ds_new;
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
+        }
+    }
+
+    long long terms_old[NM], terms_new[NM];
+    if (a.tracks) {
+        if (old != 0) {
+            const int *an = &a.anchor[(size_t)old * 4];
+            site_terms<DIM>(fold_int(x - an[0], W), fold_int(y - an[1], H), fold_int(z - an[2], D), terms_old);
+        }
+        if (nw != 0) {
+            const int *an = &a.anchor[(size_t)nw * 4];
+            site_terms<DIM>(fold_int(x - an[0], W), fold_int(y - an[1], H), fold_int(z - an[2], D), terms_new);
+        }
+        if (a.has_length) {
+            if (old != 0 && a.t.lambda_length[t_old] != 0.0)
+                delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_old, old, vol_old, terms_old, -1));
+            if (nw != 0 && a.t.lambda_length[t_new] != 0.0)
+                delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_new, nw, vol_new, terms_new, 1));
+        }
+    }
+
+    if (a.has_chemotaxis && nw != 0) {
+        const int ox = a.g.off[pick][0], oy = a.g.off[pick][1], oz = a.g.off[pick][2];
+        const uint32_t source = (uint32_t)(((size_t)wrap(z + oz, D) * H + wrap(y + oy, H)) * W + wrap(x + ox, W));
+        for (int s = 0; s < a.n_species; ++s) {
+            const float lam = a.t.chemotaxis[t_new * a.n_species + s];
+            if (lam == 0.0f) continue;
+            const float *f = a.fields[s];
+            delta = __fsub_rn(delta, __fmul_rn(lam, __fsub_rn(f[target], f[source])));
+        }
+    }
+
+    if (delta > 0.0f) {
+        const float u = to_f32(draw(a.key_accept, target));
+        if (!(u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
+    }
+
+    a.labels[target] = nw;
+    if (old != 0) {
+        atomicAdd(&a.vs_cur[old], pack_delta(-1, ds_old));
+        atomicSub(&a.vol_by_colour[(size_t)old * a.g.ncol + a.colour], 1);
+        if (a.tracks)
+#pragma unroll
+            for (int k = 0; k < NM; ++k)
+                atomicAdd(&a.mom_cur[(size_t)old * NM + k], (unsigned long long)(-terms_old[k]));
+    }
+    if (nw != 0) {
+        atomicAdd(&a.vs_cur[nw], pack_delta(1, ds_new));
+        atomicAdd(&a.vol_by_colour[(size_t)nw * a.g.ncol + a.colour], 1);
+        if (a.tracks)
+#pragma unroll
+            for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)nw * NM + k], (unsigned long long)terms_new[k]);
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ void tile_origin(int t, int W, int H, int &x0, int &y0, int &z0) {
+    using T = Tile<DIM>;
+    const int tiles_x = (W + T::TX - 1) / T::TX;
+    const int tiles_y = (H + T::TY - 1) / T::TY;
+    x0 = (t % tiles_x) * T::TX;
+    y0 = ((t / tiles_x) % tiles_y) * T::TY;
+    z0 = DIM == 3 ? (t / (tiles_x * tiles_y)) * T::TZ : 0;
+}
+
+template <int DIM>
+__device__ __forceinline__ bool tile_interior(const SweepLaunch &a, int x0, int y0, int z0) {
+    using T = Tile<DIM>;
+    return a.use_tma && x0 >= T::HX && x0 + T::TX + T::HX <= a.g.w && y0 >= 1 && y0 + T::TY + 1 <= a.g.h &&
+           (DIM == 2 || (z0 >= 1 && z0 + T::TZ + 1 <= a.g.d));
+}
+
+// One thread issues the tensor copy of a tile's window into `dst`, arriving
+// on `bar` with the byte count the copy will deliver.
+template <int DIM>
+__device__ __forceinline__ void issue_window(const CUtensorMap &tmap, uint32_t *dst, unsigned long long *bar, int x0,
+                                             int y0, int z0) {
+    using T = Tile<DIM>;
+    const uint32_t b = smem_addr(bar);
+    const uint32_t bytes = SweepSmem<DIM>::WIN * sizeof(uint32_t);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    const uint64_t map = reinterpret_cast<uint64_t>(&tmap);
+    // x0 - HX is a multiple of 4 labels, i.e. of 16 bytes, as a tensor copy's
+    // inner coordinate must be.
+    if (DIM == 2) {
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+                "r"(smem_addr(dst)),
+            "l"(map), "r"(x0 - T::HX), "r"(y0 - 1), "r"(b)
+            : "memory");
+    } else {
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+            "[%5];" ::"r"(smem_addr(dst)),
+            "l"(map), "r"(x0 - T::HX), "r"(y0 - 1), "r"(z0 - 1), "r"(b)
+            : "memory");
+    }
+}
+
+// Wait for phase `parity` of an mbarrier, giving up after kWaitLimit polls.
+__device__ __forceinline__ uint32_t wait_parity(unsigned long long *bar, uint32_t parity) {
+    const uint32_t b = smem_addr(bar);
+    uint32_t done = 0;
+    for (long long spin = 0; spin < kWaitLimit && !done; ++spin) {
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(b), "r"(parity)
+            : "memory");
+    }
+    return done;
+}
+
+template <int DIM, int NOFF>
+__global__ void __launch_bounds__(kThreads) sweep_kernel(const __grid_constant__ SweepLaunch a,
+                                                         const __grid_constant__ CUtensorMap tmap) {
+    using T = Tile<DIM>;
+    using Smem = SweepSmem<DIM>;
+    constexpr int NM = DIM == 2 ? 5 : 9;
+    static_assert(Smem::WIN_STRIDE * sizeof(uint32_t) % 128 == 0, "window buffers must stay 128-byte aligned");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // The launch asks for 128 spare bytes so the layout can start on a
+    // 128-byte boundary whatever the dynamic region's own alignment.
+    const uint32_t raw = smem_addr(smem_raw);
+    Smem &S = *reinterpret_cast<Smem *>(smem_raw + ((128u - (raw & 127u)) & 127u));
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (smem_addr(S.win[0]) & 127u) {  // never true by construction; refuse rather than copy misaligned
+        if (tid == 0) atomicExch(a.error_flag, 3);
+        return;
+    }
     const int W = a.g.w, H = a.g.h, D = a.g.d;
 
     // Tally rotation for the next pass: no thread of this pass reads what is
@@ -166,7 +433,7 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(const __grid_const
         for (size_t l = (size_t)blockIdx.x * blockDim.x + tid; l < (size_t)a.n_labels; l += stride) {
             int dv, ds;
             unpack_delta(a.vs_prev[l], dv, ds);
-            int2 b = a.vs_base[l];
+            const int2 b = a.vs_base[l];
             a.vs_next_base[l] = make_int2(b.x + dv, b.y + ds);
             a.vs_clear[l] = 0;
             if (a.tracks) {
@@ -179,252 +446,130 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(const __grid_const
         }
     }
 
-    const int tiles_x = (W + T::TX - 1) / T::TX;
-    const int tiles_y = (H + T::TY - 1) / T::TY;
-    const int bx = blockIdx.x % tiles_x;
-    const int by = (blockIdx.x / tiles_x) % tiles_y;
-    const int bz = blockIdx.x / (tiles_x * tiles_y);
-    const int x0 = bx * T::TX, y0 = by * T::TY, z0 = bz * T::TZ;
-
     const bool small_types = a.n_types <= kSmemTypes;
     if (small_types)
-        for (int i = tid; i < a.n_types * a.n_types; i += blockDim.x) s_contact[i] = a.t.contact[i];
-    if (tid < NOFF) s_woff[tid] = (a.g.off[tid][2] * T::PY + a.g.off[tid][1]) * T::PX + a.g.off[tid][0];
-    if (tid < a.g.ring_n) s_wring[tid] = (a.g.ring[tid][2] * T::PY + a.g.ring[tid][1]) * T::PX + a.g.ring[tid][0];
-
-    const bool interior = a.use_tma && x0 >= T::HX && x0 + T::TX + T::HX <= W && y0 >= 1 && y0 + T::TY + 1 <= H &&
-                          (DIM == 2 || (z0 >= 1 && z0 + T::TZ + 1 <= D));
-    bool loaded = true;
-    if (interior) {
-        // One tensor copy of the window. x0 - HX is a multiple of 4 labels,
-        // i.e. of 16 bytes, as every tensor copy's inner coordinate must be.
-        const uint32_t bar = smem_addr(&mbar);
-        if (tid == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (tid == 0) {
-            const uint32_t bytes = sizeof(win);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-            const uint64_t map = reinterpret_cast<uint64_t>(&tmap);
-            if (DIM == 2) {
-                asm volatile(
-                    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-                    "[%4];" ::"r"(smem_addr(win)),
-                    "l"(map), "r"(x0 - T::HX), "r"(y0 - 1), "r"(bar)
-                    : "memory");
-            } else {
-                asm volatile(
-                    "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
-                    "%4}], [%5];" ::"r"(smem_addr(win)),
-                    "l"(map), "r"(x0 - T::HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
-                    : "memory");
-            }
-        }
-        // Bounded wait: a copy that never lands sets the error flag and the
-        // tile is skipped rather than spinning for ever.
-        uint32_t done = 0;
-        for (long long spin = 0; spin < kWaitLimit && !done; ++spin) {
-            asm volatile(
-                "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-                : "=r"(done)
-                : "r"(bar)
-                : "memory");
-        }
-        if (!done) {
-            loaded = false;
-            if (tid == 0) atomicExch(a.error_flag, 1);
-        }
-    } else {
-        for (int i = tid; i < T::PX * T::PY * T::PZ; i += blockDim.x) {
-            const int px = i % T::PX;
-            const int py = (i / T::PX) % T::PY;
-            const int pz = i / (T::PX * T::PY);
-            const int gx = wrap(x0 - T::HX + px, W);
-            const int gy = wrap(y0 - 1 + py, H);
-            const int gz = DIM == 3 ? wrap(z0 - 1 + pz, D) : 0;
-            win[i] = a.labels[((size_t)gz * H + gy) * W + gx];
-        }
+        for (int i = tid; i < a.n_types * a.n_types; i += blockDim.x) S.contact[i] = a.t.contact[i];
+    if (tid < NOFF) S.woff[tid] = (a.g.off[tid][2] * T::PY + a.g.off[tid][1]) * T::PX + a.g.off[tid][0];
+    if (tid < a.g.ring_n) S.wring[tid] = (a.g.ring[tid][2] * T::PY + a.g.ring[tid][1]) * T::PX + a.g.ring[tid][0];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (!__syncthreads_and(loaded)) return;
 
-    const int cx = a.colour & 1, cy = (a.colour >> 1) & 1, cz = (a.colour >> 2) & 1;
-    for (int j = tid; j < T::NT; j += blockDim.x) {
-        const int jx = j % (T::TX / 2);
-        const int jy = (j / (T::TX / 2)) % (T::TY / 2);
-        const int jz = DIM == 3 ? j / ((T::TX / 2) * (T::TY / 2)) : 0;
-        const int lx = 2 * jx + cx, ly = 2 * jy + cy, lz = DIM == 3 ? 2 * jz + cz : 0;
-        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-        if (x >= W || y >= H || (DIM == 3 && z >= D)) continue;
-        const uint32_t target = (uint32_t)(((size_t)z * H + y) * W + x);
-        const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
+    const int tiles = ((W + T::TX - 1) / T::TX) * ((H + T::TY - 1) / T::TY) * (DIM == 3 ? (D + T::TZ - 1) / T::TZ : 1);
+    int waited[2] = {0, 0};
+    bool pending[2] = {false, false};  // a copy issued into the buffer and not yet waited for
+    int t = blockIdx.x;
+    if (t < tiles) {
+        int x0, y0, z0;
+        tile_origin<DIM>(t, W, H, x0, y0, z0);
+        if (tile_interior<DIM>(a, x0, y0, z0)) {
+            if (tid == 0) issue_window<DIM>(tmap, S.win[0], &S.mbar[0], x0, y0, z0);
+            pending[0] = true;
+        }
+    }
+    for (int it = 0; t < tiles; t += gridDim.x, ++it) {
+        const int buf = it & 1;
+        int x0, y0, z0;
+        tile_origin<DIM>(t, W, H, x0, y0, z0);
+        const int next = t + gridDim.x;
+        if (next < tiles) {
+            int nx0, ny0, nz0;
+            tile_origin<DIM>(next, W, H, nx0, ny0, nz0);
+            if (tile_interior<DIM>(a, nx0, ny0, nz0)) {
+                if (tid == 0) issue_window<DIM>(tmap, S.win[buf ^ 1], &S.mbar[buf ^ 1], nx0, ny0, nz0);
+                pending[buf ^ 1] = true;
+            }
+        }
+        uint32_t *win = S.win[buf];
+        if (tile_interior<DIM>(a, x0, y0, z0)) {
+            // Bounded wait: a copy that never lands sets the error flag and the
+            // CTA stops rather than spinning for ever.
+            const uint32_t done = wait_parity(&S.mbar[buf], waited[buf] & 1);
+            waited[buf] += 1;
+            pending[buf] = false;
+            if (!__syncthreads_and(done)) {
+                // Before leaving, give a copy still in flight into the other
+                // buffer its own bounded wait, so no copy lands after exit.
+                if (pending[buf ^ 1]) wait_parity(&S.mbar[buf ^ 1], waited[buf ^ 1] & 1);
+                if (tid == 0) atomicExch(a.error_flag, 1);
+                return;
+            }
+        } else {
+            for (int i = tid; i < Smem::WIN; i += blockDim.x) {
+                const int px = i % T::PX;
+                const int py = (i / T::PX) % T::PY;
+                const int pz = i / (T::PX * T::PY);
+                const int gx = wrap(x0 - T::HX + px, W);
+                const int gy = wrap(y0 - 1 + py, H);
+                const int gz = DIM == 3 ? wrap(z0 - 1 + pz, D) : 0;
+                win[i] = a.labels[((size_t)gz * H + gy) * W + gx];
+            }
+            // generic writes to a buffer a later tensor copy will overwrite
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+        }
 
-        const uint32_t old = win[wc];
-        const int pick = (int)(draw(a.key_pick, target) % (uint64_t)NOFF);
-        const uint32_t nw = win[wc + s_woff[pick]];
-        if (old == nw) continue;
-
-        const int t_old = a.cell_type[old], t_new = a.cell_type[nw];
-        float delta = 0.0f;
-        int like_old = 0, like_new = 0;
+        // Light pass: every target's pick; only targets whose neighbour
+        // carries another label are queued for pricing.
+        uint32_t *queue = S.queue[warp];
+        int count = 0;
+        constexpr int PER_LANE = Smem::TPW / 32;
 #pragma unroll
-        for (int k = 0; k < NOFF; ++k) {
-            const uint32_t ln = win[wc + s_woff[k]];
-            const int tn = ln == old ? t_old : (ln == nw ? t_new : (int)a.cell_type[ln]);
-            if (ln != old) {
-                const float j_old = small_types ? s_contact[t_old * a.n_types + tn] : a.t.contact[t_old * a.n_types + tn];
-                delta = __fsub_rn(delta, j_old);
-            } else {
-                ++like_old;
+        for (int k = 0; k < PER_LANE; ++k) {
+            const int j = warp * Smem::TPW + k * 32 + lane;
+            int lx, ly, lz;
+            target_of<DIM>(j, a.colour, lx, ly, lz);
+            const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+            bool active = false;
+            uint32_t entry = 0;
+            if (x < W && y < H && (DIM == 2 || z < D)) {
+                const uint32_t target = (uint32_t)(((size_t)z * H + y) * W + x);
+                const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
+                const int pick = (int)(draw(a.key_pick, target) % (uint64_t)NOFF);
+                active = win[wc] != win[wc + S.woff[pick]];
+                entry = (uint32_t)j | ((uint32_t)pick << 16);
             }
-            if (ln != nw) {
-                const float j_new = small_types ? s_contact[t_new * a.n_types + tn] : a.t.contact[t_new * a.n_types + tn];
-                delta = __fadd_rn(delta, j_new);
-            } else {
-                ++like_new;
-            }
+            const unsigned mask = __ballot_sync(0xffffffffu, active);
+            if (active) queue[count + __popc(mask & ((1u << lane) - 1u))] = entry;
+            count += __popc(mask);
         }
-
-        if (old != 0) {
-            // The per-colour guard: the losing cell must keep a site of
-            // another colour. A like neighbour is one, since every neighbour
-            // of a target is of another colour.
-            if (like_old == 0) {
-                int other = 0;
-                for (int c = 0; c < a.g.ncol; ++c)
-                    if (c != a.colour) other += a.vol_by_colour[(size_t)old * a.g.ncol + c];
-                if (other == 0) continue;
-            }
-            if (a.g.ring_n > 0 && a.t.connected[t_old]) {
-                uint32_t present = 0;
-                for (int k = 0; k < a.g.ring_n; ++k)
-                    if (win[wc + s_wring[k]] == old) present |= 1u << k;
-                if (!one_piece(present, a.g.adjacency)) continue;
-            }
-        }
-        const int ds_old = 2 * like_old - NOFF;
-        const int ds_new = NOFF - 2 * like_new;
-
-        int vol_old = 0, surf_old = 0, vol_new = 0, surf_new = 0;
-        if (old != 0) {
-            int dv, ds;
-            unpack_delta(a.vs_prev[old], dv, ds);
-            const int2 b = a.vs_base[old];
-            vol_old = b.x + dv;
-            surf_old = b.y + ds;
-        }
-        if (nw != 0) {
-            int dv, ds;
-            unpack_delta(a.vs_prev[nw], dv, ds);
-            const int2 b = a.vs_base[nw];
-            vol_new = b.x + dv;
-            surf_new = b.y + ds;
-        }
-        if (old != 0) {
-            const float lam = a.t.lambda_volume[t_old];
-            if (lam != 0.0f) {
-                const float v = (float)vol_old, tv = a.t.target_volume[t_old];
-                const float p = __fsub_rn(__fsub_rn(v, 1.0f), tv), q = __fsub_rn(v, tv);
-                delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(__fmul_rn(p, p), __fmul_rn(q, q))));
-            }
-        }
-        if (nw != 0) {
-            const float lam = a.t.lambda_volume[t_new];
-            if (lam != 0.0f) {
-                const float v = (float)vol_new, tv = a.t.target_volume[t_new];
-                const float p = __fsub_rn(__fadd_rn(v, 1.0f), tv), q = __fsub_rn(v, tv);
-                delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(__fmul_rn(p, p), __fmul_rn(q, q))));
-            }
-        }
-        if (old != 0) {
-            const float lam = a.t.lambda_surface[t_old];
-            if (lam != 0.0f) {
-                const float sv = (float)surf_old, ts = a.t.target_surface[t_old];
-                const float after = __fadd_rn(sv, (float)ds_old);
-                const float p = __fsub_rn(after, ts), q = __fsub_rn(sv, ts);
-                delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(__fmul_rn(p, p), __fmul_rn(q, q))));
-            }
-        }
-        if (nw != 0) {
-            const float lam = a.t.lambda_surface[t_new];
-            if (lam != 0.0f) {
-                const float sv = (float)surf_new, ts = a.t.target_surface[t_new];
-                const float after = __fadd_rn(sv, (float)ds_new);
-                const float p = __fsub_rn(after, ts), q = __fsub_rn(sv, ts);
-                delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(__fmul_rn(p, p), __fmul_rn(q, q))));
-            }
-        }
-
-        long long terms_old[NM], terms_new[NM];
-        if (a.tracks) {
-            if (old != 0) {
-                const int *an = &a.anchor[(size_t)old * 4];
-                site_terms<DIM>(fold_int(x - an[0], W), fold_int(y - an[1], H), fold_int(z - an[2], D), terms_old);
-            }
-            if (nw != 0) {
-                const int *an = &a.anchor[(size_t)nw * 4];
-                site_terms<DIM>(fold_int(x - an[0], W), fold_int(y - an[1], H), fold_int(z - an[2], D), terms_new);
-            }
-            if (a.has_length) {
-                if (old != 0 && a.t.lambda_length[t_old] != 0.0)
-                    delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_old, old, vol_old, terms_old, -1));
-                if (nw != 0 && a.t.lambda_length[t_new] != 0.0)
-                    delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_new, nw, vol_new, terms_new, 1));
-            }
-        }
-
-        if (a.has_chemotaxis && nw != 0) {
-            const int ox = a.g.off[pick][0], oy = a.g.off[pick][1], oz = a.g.off[pick][2];
-            const uint32_t source =
-                (uint32_t)(((size_t)wrap(z + oz, D) * H + wrap(y + oy, H)) * W + wrap(x + ox, W));
-            for (int s = 0; s < a.n_species; ++s) {
-                const float lam = a.t.chemotaxis[t_new * a.n_species + s];
-                if (lam == 0.0f) continue;
-                const float *f = a.fields[s];
-                delta = __fsub_rn(delta, __fmul_rn(lam, __fsub_rn(f[target], f[source])));
-            }
-        }
-
-        bool accept = delta <= 0.0f;
-        if (!accept) {
-            const float u = to_f32(draw(a.key_accept, target));
-            accept = u < metropolis_exp(__fdiv_rn(-delta, a.temperature));
-        }
-        if (!accept) continue;
-
-        a.labels[target] = nw;
-        if (old != 0) {
-            atomicAdd(&a.vs_cur[old], pack_delta(-1, ds_old));
-            atomicSub(&a.vol_by_colour[(size_t)old * a.g.ncol + a.colour], 1);
-            if (a.tracks)
-#pragma unroll
-                for (int k = 0; k < NM; ++k)
-                    atomicAdd(&a.mom_cur[(size_t)old * NM + k], (unsigned long long)(-terms_old[k]));
-        }
-        if (nw != 0) {
-            atomicAdd(&a.vs_cur[nw], pack_delta(1, ds_new));
-            atomicAdd(&a.vol_by_colour[(size_t)nw * a.g.ncol + a.colour], 1);
-            if (a.tracks)
-#pragma unroll
-                for (int k = 0; k < NM; ++k)
-                    atomicAdd(&a.mom_cur[(size_t)nw * NM + k], (unsigned long long)terms_new[k]);
-        }
+        __syncwarp();
+        // Heavy pass: the queued copies, one per lane.
+        for (int e = lane; e < count; e += 32)
+            price_and_commit<DIM, NOFF>(a, S, win, queue[e], x0, y0, z0, small_types);
+        __syncthreads();
     }
 }
 
 template <int DIM, int NOFF>
 static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
     using T = Tile<DIM>;
+    static int grid_cap = 0;
+    const size_t smem = sizeof(SweepSmem<DIM>) + 128;
+    if (!grid_cap) {
+        cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIM, NOFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e) return e;
+        int dev = 0, sms = 0, per_sm = 0;
+        if ((e = cudaGetDevice(&dev))) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<DIM, NOFF>, kThreads, smem)))
+            return e;
+        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
+    }
     const int tiles = ((a.g.w + T::TX - 1) / T::TX) * ((a.g.h + T::TY - 1) / T::TY) *
                       (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
+    int grid = tiles < grid_cap ? tiles : grid_cap;
+    if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
     CUtensorMap tmap;
     if (a.use_tma && a.tensor_map)
         tmap = *static_cast<const CUtensorMap *>(a.tensor_map);
     else
         memset(&tmap, 0, sizeof tmap);
-    sweep_kernel<DIM, NOFF><<<tiles, kSweepThreads, 0, stream>>>(a, tmap);
+    sweep_kernel<DIM, NOFF><<<grid, kThreads, smem, stream>>>(a, tmap);
     return cudaGetLastError();
 }
 
@@ -440,8 +585,7 @@ cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream) {
     return cudaErrorInvalidValue;
 }
 
-// The tensor map a sweep's interior tiles copy their window with: the
-// lattice as a 2D or 3D uint32 array, a box of the tile plus its halo.
+// The box a sweep tile's tensor copy moves: the tile plus its halo.
 int sweep_box(int dim, uint32_t box[3]) {
     if (dim == 2) {
         box[0] = Tile<2>::PX;

@@ -160,7 +160,7 @@ typedef struct {
     int ring_n, ring[26][3];
     uint32_t adjacency[26];
     int n_types, n_species;
-    float temperature;
+    float beta; /* (float)(1 / T), rounded once on the host */
     uint64_t seed;
     float *contact, *tv, *lv, *ts, *ls, *chemo, *sec, *upt;
     double *tl, *ll, *div_vol, *death;
@@ -284,7 +284,7 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
     int nt = m->n_types, ns = m->n_species;
     s->n_types = nt;
     s->n_species = ns;
-    s->temperature = (float)m->temperature;
+    s->beta = (float)(1.0 / m->temperature);
     s->seed = m->seed;
     s->contact = f32_copy(m->contact, (size_t)nt * nt);
     s->tv = f32_copy(m->target_volume, nt);
@@ -503,27 +503,23 @@ static void pass(rsim *s, int colour) {
                 int ds_old = 2 * like_old - bonds;
                 int ds_new = bonds - 2 * like_new;
 
+                /* lambda ((v -/+ 1 - V_t)^2 - (v - V_t)^2) = lambda (1 -/+ 2 (v - V_t)) */
                 if (old != 0 && s->lv[t_old] != 0.0f) {
-                    float v = (float)snap_vol[old], tv = s->tv[t_old];
-                    float a = v - 1.0f - tv, b = v - tv;
-                    delta = delta + s->lv[t_old] * (a * a - b * b);
+                    float dv = (float)snap_vol[old] - s->tv[t_old];
+                    delta = delta + s->lv[t_old] * (1.0f - 2.0f * dv);
                 }
                 if (nw != 0 && s->lv[t_new] != 0.0f) {
-                    float v = (float)snap_vol[nw], tv = s->tv[t_new];
-                    float a = v + 1.0f - tv, b = v - tv;
-                    delta = delta + s->lv[t_new] * (a * a - b * b);
+                    float dv = (float)snap_vol[nw] - s->tv[t_new];
+                    delta = delta + s->lv[t_new] * (2.0f * dv + 1.0f);
                 }
+                /* lambda ((s + ds - S_t)^2 - (s - S_t)^2) = lambda ds (2 (s - S_t) + ds) */
                 if (old != 0 && s->ls[t_old] != 0.0f) {
-                    float sv = (float)snap_surf[old], ts = s->ts[t_old];
-                    float after = sv + (float)ds_old;
-                    float a = after - ts, b = sv - ts;
-                    delta = delta + s->ls[t_old] * (a * a - b * b);
+                    float e = (float)snap_surf[old] - s->ts[t_old], dsf = (float)ds_old;
+                    delta = delta + s->ls[t_old] * (dsf * (2.0f * e + dsf));
                 }
                 if (nw != 0 && s->ls[t_new] != 0.0f) {
-                    float sv = (float)snap_surf[nw], ts = s->ts[t_new];
-                    float after = sv + (float)ds_new;
-                    float a = after - ts, b = sv - ts;
-                    delta = delta + s->ls[t_new] * (a * a - b * b);
+                    float e = (float)snap_surf[nw] - s->ts[t_new], dsf = (float)ds_new;
+                    delta = delta + s->ls[t_new] * (dsf * (2.0f * e + dsf));
                 }
                 int64_t terms_old[9], terms_new[9];
                 if (s->tracks) {
@@ -556,7 +552,7 @@ static void pass(rsim *s, int colour) {
                 int accept = delta <= 0.0f;
                 if (!accept) {
                     float u = to_f32(draw(s->seed, target, step, colour, 1));
-                    accept = u < rp_expf(-delta / s->temperature);
+                    accept = u < rp_expf(-delta * s->beta);
                 }
                 if (!accept) continue;
                 s->accepted += 1;

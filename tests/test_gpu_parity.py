@@ -3,8 +3,9 @@
 Every case runs the same start on the B200 (through the C ABI) and on the
 replay (oracle/replay.c) and requires identical labels, per-label volumes,
 surfaces and cell types, and bit-identical f32 fields. Each case runs with
-the sweep's tensor-copy window load on and off, so both load paths are held
-to the same result.
+the sweep's tensor-copy window load on and off, and with the persistent grid
+at its default and capped at three CTAs (each CTA then walks several tiles
+through both window buffers), so every load path is held to one result.
 """
 
 from __future__ import annotations
@@ -34,7 +35,9 @@ def _von_neumann():
 
 
 def _large():
-    m = sheet_model(width=256, height=192, seed=2, contact=(0, 10, 10, 10), lambda_volume=1.0,
+    # 384 x 192: the tiles at x0 = 128, y0 = 32..128 lie clear of the periodic
+    # edge, so their windows arrive by tensor copy
+    m = sheet_model(width=384, height=192, seed=2, contact=(0, 10, 10, 10), lambda_volume=1.0,
                     target_surface=92.0, lambda_surface=0.2)
     return tiled(m), 10
 
@@ -58,7 +61,8 @@ def _volume(order):
 
 
 def _volume_wide():
-    m = sheet_model(width=96, height=32, depth=32, seed=8, target_volume=512.0, order=3, contact=(0, 10, 10, 10),
+    # 192 x 32 x 32: four tiles lie clear of the edge and take tensor copies
+    m = sheet_model(width=192, height=32, depth=32, seed=8, target_volume=512.0, order=3, contact=(0, 10, 10, 10),
                     lambda_volume=1.0)
     return tiled(m), 4
 
@@ -120,12 +124,16 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("ctas", ["0", "3"])
 @pytest.mark.parametrize("tma", ["1", "0"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, monkeypatch):
+def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, monkeypatch):
+    """`ctas` 3 caps the sweep's persistent grid at three CTAs, so every CTA
+    walks several tiles and both window buffers take tensor copies."""
     made, steps = CASES[name]()
     start, fields = made if isinstance(made, tuple) else (made, None)
     monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
+    monkeypatch.setenv("GLAZIER_SWEEP_CTAS", ctas)
     gpu = device.GpuSimulation.from_start(start, fields)
     replay = ReplayOracle.from_start(start, fields)
     for chunk in (1, steps - 1):
