@@ -124,6 +124,10 @@ struct glz_gpu {
     uint64_t pass_no = 0, mcs = 0;
     bool use_tma = false;
     int max_ctas = 0;
+    int uniform = -1;
+    bool uniform_exact = false;
+    float uniform_j = 0.0f;
+    std::vector<float> host_tv, host_lv, host_ts, host_ls;
     CUtensorMap tmap{};
     int *error_flag = nullptr;
     unsigned long long *medium = nullptr;
@@ -273,6 +277,29 @@ int settle(glz_gpu *h) {
     return GLZ_OK;
 }
 
+// The one type every label carries, or -1 when labels differ in type. The
+// reference gives the medium's entry the first cell type (cpu.rs:203), so a
+// single-type tissue is uniform medium included. Set at creation; a daughter
+// takes its mother's type, so division keeps it.
+void find_uniform_type(glz_gpu *h, const double *contact, int n_types) {
+    h->uniform = -1;
+    if (h->n_labels == 0) return;
+    const uint8_t t = h->cell_type_host[0];
+    for (size_t l = 1; l < h->n_labels; ++l)
+        if (h->cell_type_host[l] != t) return;
+    h->uniform = t;
+    // The sweep then sums contact energies as J times a count m, |m| <=
+    // n_off, which equals the neighbour-by-neighbour f32 sum when every J m
+    // is exactly representable in f32.
+    const float j = (float)contact[t * n_types + t];
+    h->uniform_j = j;
+    h->uniform_exact = true;
+    for (int m = -26; m <= 26; ++m) {
+        const double exact = (double)j * (double)m;
+        if ((double)(float)exact != exact) h->uniform_exact = false;
+    }
+}
+
 int sweep_pass(glz_gpu *h, int colour) {
     const uint64_t p = h->pass_no;
     glz::SweepLaunch a{};
@@ -300,6 +327,15 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.vol_by_colour = h->t.vol_by_colour;
     a.anchor = h->t.anchor;
     a.n_labels = (int)h->n_labels;
+    a.uniform_type = h->uniform;
+    a.uniform_contact_exact = h->uniform_exact;
+    a.uniform_contact = h->uniform_j;
+    if (h->uniform >= 0) {
+        a.u_target_volume = h->host_tv[h->uniform];
+        a.u_lambda_volume = h->host_lv[h->uniform];
+        a.u_target_surface = h->host_ts[h->uniform];
+        a.u_lambda_surface = h->host_ls[h->uniform];
+    }
     a.has_length = h->has_length;
     a.tracks = h->tracks;
     a.has_chemotaxis = h->has_chemotaxis;
@@ -548,6 +584,10 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         }
     }
 
+    h->host_tv = tv;
+    h->host_lv = lv;
+    h->host_ts = ts;
+    h->host_ls = ls;
     int rc;
     if ((rc = upload(h, &h->contact, contact)) || (rc = upload(h, &h->tv, tv)) || (rc = upload(h, &h->lv, lv)) ||
         (rc = upload(h, &h->ts, ts)) || (rc = upload(h, &h->ls, ls)) || (rc = upload(h, &h->tl, tl)) ||
@@ -561,6 +601,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         return bail(fail(GLZ_DRIVER, "label upload failed"));
     h->cell_type_host.assign(cell_type, cell_type + n_labels);
     h->n_labels = n_labels;
+    find_uniform_type(h, m->contact, nt);
     if ((rc = alloc_labels(h, h->has_pop ? 2 * n_labels + 16 : n_labels))) return bail(rc);
 
     if (ns > 0) {

@@ -72,6 +72,10 @@ struct SweepLaunch {
     int *vol_by_colour;
     const int *anchor;
     int n_labels;
+    int uniform_type;  // the type of every label when they share one, else -1
+    int uniform_contact_exact;  // J m is exact in f32 for every |m| <= n_off (see sweep.cu)
+    float uniform_contact;      // J[type][type] when uniform
+    float u_target_volume, u_lambda_volume, u_target_surface, u_lambda_surface;
     int has_length, tracks, has_chemotaxis;
     const float *fields[kMaxSpecies];
     int use_tma;

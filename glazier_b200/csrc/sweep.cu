@@ -12,11 +12,12 @@
 //     buffers, so the copy of tile i+1 overlaps the work on tile i. Edge
 //     tiles, and lattices whose rows are not whole 16-byte units, take
 //     wrapped plain loads.
-//   - Each warp first draws every target's neighbour pick (one counter-hash
+//   - The CTA first draws every target's neighbour pick (one counter-hash
 //     draw per target) and keeps only the targets whose neighbour carries
-//     another label, about a fifth of them in a tissue, in a per-warp queue;
-//     it then prices the queued copies densely, one per lane. The expensive
-//     path never runs with idle lanes that a light target left behind.
+//     another label, about a fifth of them in a tissue, in a shared queue;
+//     warps then take the queue 32 copies at a time and price them densely.
+//     The expensive path never runs with idle lanes that a light target left
+//     behind, and no warp waits on another's share.
 //
 // Per-cell tallies (volume, surface, exact moment sums) are read from the
 // snapshot the rotation in engine.h gives each pass and changed by integer
@@ -51,6 +52,46 @@ struct Tile<3> {
     static constexpr int NT = (TX / 2) * (TY / 2) * (TZ / 2);
 };
 
+// The neighbour offsets of each neighbourhood in the reference's order
+// (lattice.rs:8-88): a plane takes ORDER1's four in-plane faces or ORDER3's
+// eight in-plane neighbours; a volume takes ORDER1, ORDER2 or ORDER3 whole.
+// The host builds the same table (engine.cu) and the launch checks they agree.
+template <int DIM, int NOFF>
+__host__ __device__ constexpr int neighbour_offset(int k, int axis) {
+    if (DIM == 2 && NOFF == 4) {
+        constexpr int o[4][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}};
+        return o[k][axis];
+    }
+    if (DIM == 2 && NOFF == 8) {
+        constexpr int o[8][3] = {{-1, -1, 0}, {0, -1, 0}, {1, -1, 0}, {-1, 0, 0},
+                                 {1, 0, 0},   {-1, 1, 0}, {0, 1, 0},  {1, 1, 0}};
+        return o[k][axis];
+    }
+    if (DIM == 3 && NOFF == 6) {
+        constexpr int o[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        return o[k][axis];
+    }
+    if (DIM == 3 && NOFF == 18) {
+        constexpr int o[18][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},   {0, -1, 0}, {0, 0, 1},  {0, 0, -1},
+                                  {1, 1, 0},  {1, -1, 0}, {-1, 1, 0},  {-1, -1, 0}, {1, 0, 1}, {1, 0, -1},
+                                  {-1, 0, 1}, {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1}, {0, -1, -1}};
+        return o[k][axis];
+    }
+    // ORDER3: dz, then dy, then dx from -1 to 1, the centre left out
+    const int kk = k < 13 ? k : k + 1;
+    return axis == 0 ? kk % 3 - 1 : (axis == 1 ? (kk / 3) % 3 - 1 : kk / 9 - 1);
+}
+
+template <int DIM, int NOFF>
+__host__ __device__ constexpr int window_offset(int k) {
+    return (neighbour_offset<DIM, NOFF>(k, 2) * Tile<DIM>::PY + neighbour_offset<DIM, NOFF>(k, 1)) * Tile<DIM>::PX +
+           neighbour_offset<DIM, NOFF>(k, 0);
+}
+
+#ifndef GLZ_SWEEP_MIN_BLOCKS
+#define GLZ_SWEEP_MIN_BLOCKS 4
+#endif
+
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kSmemTypes = 16;  // contact tables up to 16 types live in shared memory
@@ -64,7 +105,8 @@ struct SweepSmem {
     static constexpr int WIN_STRIDE = (WIN + 31) / 32 * 32;
     static constexpr int TPW = Tile<DIM>::NT / kWarps;  // targets per warp per tile
     alignas(128) uint32_t win[2][WIN_STRIDE];
-    uint32_t queue[kWarps][TPW];
+    uint32_t queue[Tile<DIM>::NT];  // the tile's targets whose neighbour carries another label
+    int queued, taken;
     float contact[kSmemTypes * kSmemTypes];
     int woff[26];
     int wring[26];
@@ -184,8 +226,12 @@ __device__ __forceinline__ void target_of(int j, int colour, int &lx, int &ly, i
 }
 
 // Price one copy attempt whose neighbour pick is known to carry another label
-// and commit it if the Metropolis test takes it.
-template <int DIM, int NOFF>
+// and commit it if the Metropolis test takes it. UNIFORM: every label carries
+// one type, so the contact sum is J times a difference of like-neighbour
+// counts (the host has checked that J m is exact in f32 for every count m,
+// which makes it the same number the neighbour-by-neighbour sum rounds to)
+// and the per-type constants come from the launch parameters.
+template <int DIM, int NOFF, bool UNIFORM>
 __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const SweepSmem<DIM> &S, const uint32_t *win,
                                                  uint32_t entry, int x0, int y0, int z0, bool small_types) {
     using T = Tile<DIM>;
@@ -213,25 +259,38 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
         base_new = a.vs_base[nw];
         prev_new = a.vs_prev[nw];
     }
-    const int t_old = a.cell_type[old], t_new = a.cell_type[nw];
+    const int t_old = UNIFORM ? a.uniform_type : a.cell_type[old];
+    const int t_new = UNIFORM ? a.uniform_type : a.cell_type[nw];
 
     float delta = 0.0f;
     int like_old = 0, like_new = 0;
+    if (UNIFORM) {
 #pragma unroll
-    for (int k = 0; k < NOFF; ++k) {
-        const uint32_t ln = win[wc + S.woff[k]];
-        const int tn = ln == old ? t_old : (ln == nw ? t_new : (int)a.cell_type[ln]);
-        if (ln != old) {
-            const float j_old = small_types ? S.contact[t_old * a.n_types + tn] : a.t.contact[t_old * a.n_types + tn];
-            delta = __fsub_rn(delta, j_old);
-        } else {
-            ++like_old;
+        for (int k = 0; k < NOFF; ++k) {
+            const uint32_t ln = win[wc + window_offset<DIM, NOFF>(k)];
+            like_old += ln == old;
+            like_new += ln == nw;
         }
-        if (ln != nw) {
-            const float j_new = small_types ? S.contact[t_new * a.n_types + tn] : a.t.contact[t_new * a.n_types + tn];
-            delta = __fadd_rn(delta, j_new);
-        } else {
-            ++like_new;
+        delta = __fmul_rn(a.uniform_contact, (float)(like_old - like_new));
+    } else {
+#pragma unroll
+        for (int k = 0; k < NOFF; ++k) {
+            const uint32_t ln = win[wc + window_offset<DIM, NOFF>(k)];
+            const int tn = ln == old ? t_old : (ln == nw ? t_new : (int)a.cell_type[ln]);
+            if (ln != old) {
+                const float j_old =
+                    small_types ? S.contact[t_old * a.n_types + tn] : a.t.contact[t_old * a.n_types + tn];
+                delta = __fsub_rn(delta, j_old);
+            } else {
+                ++like_old;
+            }
+            if (ln != nw) {
+                const float j_new =
+                    small_types ? S.contact[t_new * a.n_types + tn] : a.t.contact[t_new * a.n_types + tn];
+                delta = __fadd_rn(delta, j_new);
+            } else {
+                ++like_new;
+            }
         }
     }
 
@@ -267,31 +326,33 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
     }
     // lambda ((v -/+ 1 - V_t)^2 - (v - V_t)^2) = lambda (1 -/+ 2 (v - V_t))
     if (old != 0) {
-        const float lam = a.t.lambda_volume[t_old];
+        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_old];
         if (lam != 0.0f) {
-            const float dv = __fsub_rn((float)vol_old, a.t.target_volume[t_old]);
+            const float dv = __fsub_rn((float)vol_old, UNIFORM ? a.u_target_volume : a.t.target_volume[t_old]);
             delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, dv))));
         }
     }
     if (nw != 0) {
-        const float lam = a.t.lambda_volume[t_new];
+        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_new];
         if (lam != 0.0f) {
-            const float dv = __fsub_rn((float)vol_new, a.t.target_volume[t_new]);
+            const float dv = __fsub_rn((float)vol_new, UNIFORM ? a.u_target_volume : a.t.target_volume[t_new]);
             delta = __fadd_rn(delta, __fmul_rn(lam, __fadd_rn(__fmul_rn(2.0f, dv), 1.0f)));
         }
     }
     // lambda ((s + ds - S_t)^2 - (s - S_t)^2) = lambda ds (2 (s - S_t) + ds)
     if (old != 0) {
-        const float lam = a.t.lambda_surface[t_old];
+        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_old];
         if (lam != 0.0f) {
-            const float e = __fsub_rn((float)surf_old, a.t.target_surface[t_old]), dsf = (float)ds_old;
+            const float e = __fsub_rn((float)surf_old, UNIFORM ? a.u_target_surface : a.t.target_surface[t_old]);
+            const float dsf = (float)ds_old;
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
         }
     }
     if (nw != 0) {
-        const float lam = a.t.lambda_surface[t_new];
+        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_new];
         if (lam != 0.0f) {
-            const float e = __fsub_rn((float)surf_new, a.t.target_surface[t_new]), dsf = (float)ds_new;
+            const float e = __fsub_rn((float)surf_new, UNIFORM ? a.u_target_surface : a.t.target_surface[t_new]);
+            const float dsf = (float)ds_new;
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
         }
     }
@@ -406,8 +467,8 @@ __device__ __forceinline__ uint32_t wait_parity(unsigned long long *bar, uint32_
     return done;
 }
 
-template <int DIM, int NOFF>
-__global__ void __launch_bounds__(kThreads) sweep_kernel(const __grid_constant__ SweepLaunch a,
+template <int DIM, int NOFF, bool UNIFORM>
+__global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(const __grid_constant__ SweepLaunch a,
                                                          const __grid_constant__ CUtensorMap tmap) {
     using T = Tile<DIM>;
     using Smem = SweepSmem<DIM>;
@@ -452,6 +513,8 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const __grid_constant__
     if (tid < NOFF) S.woff[tid] = (a.g.off[tid][2] * T::PY + a.g.off[tid][1]) * T::PX + a.g.off[tid][0];
     if (tid < a.g.ring_n) S.wring[tid] = (a.g.ring[tid][2] * T::PY + a.g.ring[tid][1]) * T::PX + a.g.ring[tid][0];
     if (tid == 0) {
+        S.queued = 0;
+        S.taken = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[0])));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[1])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -498,13 +561,23 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const __grid_constant__
                 return;
             }
         } else {
+            // A lattice at least a window wide wraps each coordinate at most
+            // once, by a compare; a smaller one takes the remainder.
+            const bool once = W >= T::PX && H >= T::PY && (DIM == 2 || D >= T::PZ);
             for (int i = tid; i < Smem::WIN; i += blockDim.x) {
                 const int px = i % T::PX;
                 const int py = (i / T::PX) % T::PY;
                 const int pz = i / (T::PX * T::PY);
-                const int gx = wrap(x0 - T::HX + px, W);
-                const int gy = wrap(y0 - 1 + py, H);
-                const int gz = DIM == 3 ? wrap(z0 - 1 + pz, D) : 0;
+                int gx = x0 - T::HX + px, gy = y0 - 1 + py, gz = DIM == 3 ? z0 - 1 + pz : 0;
+                if (once) {
+                    gx += gx < 0 ? W : (gx >= W ? -W : 0);
+                    gy += gy < 0 ? H : (gy >= H ? -H : 0);
+                    if (DIM == 3) gz += gz < 0 ? D : (gz >= D ? -D : 0);
+                } else {
+                    gx = wrap(gx, W);
+                    gy = wrap(gy, H);
+                    gz = DIM == 3 ? wrap(gz, D) : 0;
+                }
                 win[i] = a.labels[((size_t)gz * H + gy) * W + gx];
             }
             // generic writes to a buffer a later tensor copy will overwrite
@@ -513,9 +586,7 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const __grid_constant__
         }
 
         // Light pass: every target's pick; only targets whose neighbour
-        // carries another label are queued for pricing.
-        uint32_t *queue = S.queue[warp];
-        int count = 0;
+        // carries another label go into the tile's queue.
         constexpr int PER_LANE = Smem::TPW / 32;
 #pragma unroll
         for (int k = 0; k < PER_LANE; ++k) {
@@ -533,30 +604,47 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(const __grid_constant__
                 entry = (uint32_t)j | ((uint32_t)pick << 16);
             }
             const unsigned mask = __ballot_sync(0xffffffffu, active);
-            if (active) queue[count + __popc(mask & ((1u << lane) - 1u))] = entry;
-            count += __popc(mask);
+            int base = 0;
+            if (lane == 0 && mask) base = atomicAdd(&S.queued, __popc(mask));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (active) S.queue[base + __popc(mask & ((1u << lane) - 1u))] = entry;
         }
-        __syncwarp();
-        // Heavy pass: the queued copies, one per lane.
-        for (int e = lane; e < count; e += 32)
-            price_and_commit<DIM, NOFF>(a, S, win, queue[e], x0, y0, z0, small_types);
         __syncthreads();
+        // Heavy pass: warps take the queue 32 copies at a time.
+        const int queued = S.queued;
+        for (;;) {
+            int first = 0;
+            if (lane == 0) first = atomicAdd(&S.taken, 32);
+            first = __shfl_sync(0xffffffffu, first, 0);
+            if (first >= queued) break;
+            if (first + lane < queued)
+                price_and_commit<DIM, NOFF, UNIFORM>(a, S, win, S.queue[first + lane], x0, y0, z0, small_types);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            S.queued = 0;
+            S.taken = 0;
+        }
     }
 }
 
-template <int DIM, int NOFF>
+template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
+    // the compile-time neighbourhood must be the one the host built
+    for (int k = 0; k < NOFF; ++k)
+        for (int axis = 0; axis < 3; ++axis)
+            if (a.g.off[k][axis] != neighbour_offset<DIM, NOFF>(k, axis)) return cudaErrorInvalidValue;
     using T = Tile<DIM>;
     static int grid_cap = 0;
     const size_t smem = sizeof(SweepSmem<DIM>) + 128;
     if (!grid_cap) {
-        cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIM, NOFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIM, NOFF, UNIFORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e) return e;
         int dev = 0, sms = 0, per_sm = 0;
         if ((e = cudaGetDevice(&dev))) return e;
         if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<DIM, NOFF>, kThreads, smem)))
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<DIM, NOFF, UNIFORM>, kThreads, smem)))
             return e;
         grid_cap = sms * (per_sm > 0 ? per_sm : 1);
     }
@@ -569,20 +657,25 @@ static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
         tmap = *static_cast<const CUtensorMap *>(a.tensor_map);
     else
         memset(&tmap, 0, sizeof tmap);
-    sweep_kernel<DIM, NOFF><<<grid, kThreads, smem, stream>>>(a, tmap);
+    sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kThreads, smem, stream>>>(a, tmap);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream) {
+template <bool UNIFORM>
+static cudaError_t launch_any(const SweepLaunch &a, cudaStream_t stream) {
     if (a.g.dim == 2) {
-        if (a.g.n_off == 4) return launch<2, 4>(a, stream);
-        if (a.g.n_off == 8) return launch<2, 8>(a, stream);
+        if (a.g.n_off == 4) return launch<2, 4, UNIFORM>(a, stream);
+        if (a.g.n_off == 8) return launch<2, 8, UNIFORM>(a, stream);
     } else {
-        if (a.g.n_off == 6) return launch<3, 6>(a, stream);
-        if (a.g.n_off == 18) return launch<3, 18>(a, stream);
-        if (a.g.n_off == 26) return launch<3, 26>(a, stream);
+        if (a.g.n_off == 6) return launch<3, 6, UNIFORM>(a, stream);
+        if (a.g.n_off == 18) return launch<3, 18, UNIFORM>(a, stream);
+        if (a.g.n_off == 26) return launch<3, 26, UNIFORM>(a, stream);
     }
     return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream) {
+    return a.uniform_type >= 0 && a.uniform_contact_exact ? launch_any<true>(a, stream) : launch_any<false>(a, stream);
 }
 
 // The box a sweep tile's tensor copy moves: the tile plus its halo.
