@@ -89,7 +89,7 @@ __host__ __device__ constexpr int window_offset(int k) {
 }
 
 #ifndef GLZ_SWEEP_MIN_BLOCKS
-#define GLZ_SWEEP_MIN_BLOCKS 4
+#define GLZ_SWEEP_MIN_BLOCKS 3
 #endif
 
 constexpr int kThreads = 256;
@@ -225,6 +225,83 @@ __device__ __forceinline__ void target_of(int j, int colour, int &lx, int &ly, i
     lz = DIM == 3 ? 2 * jz + ((colour >> 2) & 1) : 0;
 }
 
+// The rare parts of pricing live out of line, so the registers they need do
+// not weigh on the common path.
+
+// The per-colour guard: whether cell `old` keeps a site of a colour other than
+// the pass's own, which no copy in this pass can take.
+__device__ __noinline__ bool keeps_other_colour(const SweepLaunch &a, uint32_t old) {
+    int other = 0;
+    for (int c = 0; c < a.g.ncol; ++c)
+        if (c != a.colour) other += a.vol_by_colour[(size_t)old * a.g.ncol + c];
+    return other != 0;
+}
+
+// The connectivity veto (lib.rs:511-521): the ring positions of `old` around
+// the target must be one piece.
+__device__ __noinline__ bool ring_one_piece(const SweepLaunch &a, const int *wring, const uint32_t *win, int wc,
+                                            uint32_t old) {
+    uint32_t present = 0;
+    for (int k = 0; k < a.g.ring_n; ++k)
+        if (win[wc + wring[k]] == old) present |= 1u << k;
+    return one_piece(present, a.g.adjacency);
+}
+
+// The moment-sum terms of the target site in a cell's own frame.
+template <int DIM>
+__device__ __forceinline__ void terms_of(const SweepLaunch &a, uint32_t label, int x, int y, int z, long long *t) {
+    const int *an = &a.anchor[(size_t)label * 4];
+    site_terms<DIM>(fold_int(x - an[0], a.g.w), fold_int(y - an[1], a.g.h), fold_int(z - an[2], a.g.d), t);
+}
+
+// The length and chemotaxis terms of a copy (cpu.rs:291-305, 381-395).
+template <int DIM>
+__device__ __noinline__ float extra_terms(const SweepLaunch &a, uint32_t old, uint32_t nw, int t_old, int t_new,
+                                          int vol_old, int vol_new, int x, int y, int z, int pick, uint32_t target,
+                                          float delta) {
+    constexpr int NM = DIM == 2 ? 5 : 9;
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    if (a.has_length) {
+        long long terms[NM];
+        if (old != 0 && a.t.lambda_length[t_old] != 0.0) {
+            terms_of<DIM>(a, old, x, y, z, terms);
+            delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_old, old, vol_old, terms, -1));
+        }
+        if (nw != 0 && a.t.lambda_length[t_new] != 0.0) {
+            terms_of<DIM>(a, nw, x, y, z, terms);
+            delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_new, nw, vol_new, terms, 1));
+        }
+    }
+    if (a.has_chemotaxis && nw != 0) {
+        const int ox = a.g.off[pick][0], oy = a.g.off[pick][1], oz = a.g.off[pick][2];
+        const uint32_t source = (uint32_t)(((size_t)wrap(z + oz, D) * H + wrap(y + oy, H)) * W + wrap(x + ox, W));
+        for (int s = 0; s < a.n_species; ++s) {
+            const float lam = a.t.chemotaxis[t_new * a.n_species + s];
+            if (lam == 0.0f) continue;
+            const float *f = a.fields[s];
+            delta = __fsub_rn(delta, __fmul_rn(lam, __fsub_rn(f[target], f[source])));
+        }
+    }
+    return delta;
+}
+
+// The moment sums follow an accepted copy: the site leaves `old` and joins `nw`.
+template <int DIM>
+__device__ __noinline__ void commit_moments(const SweepLaunch &a, uint32_t old, uint32_t nw, int x, int y, int z) {
+    constexpr int NM = DIM == 2 ? 5 : 9;
+    long long terms[NM];
+    if (old != 0) {
+        terms_of<DIM>(a, old, x, y, z, terms);
+#pragma unroll
+        for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)old * NM + k], (unsigned long long)(-terms[k]));
+    }
+    if (nw != 0) {
+        terms_of<DIM>(a, nw, x, y, z, terms);
+#pragma unroll
+        for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)nw * NM + k], (unsigned long long)terms[k]);
+    }
+}
+
 // Price one copy attempt whose neighbour pick is known to carry another label
 // and commit it if the Metropolis test takes it. UNIFORM: every label carries
 // one type, so the contact sum is J times a difference of like-neighbour
@@ -235,14 +312,13 @@ template <int DIM, int NOFF, bool UNIFORM>
 __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const SweepSmem<DIM> &S, const uint32_t *win,
                                                  uint32_t entry, int x0, int y0, int z0, bool small_types) {
     using T = Tile<DIM>;
-    constexpr int NM = DIM == 2 ? 5 : 9;
-    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    const int W = a.g.w, H = a.g.h;
     const int j = (int)(entry & 0xffffu);
     const int pick = (int)(entry >> 16);
     int lx, ly, lz;
     target_of<DIM>(j, a.colour, lx, ly, lz);
     const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-    const uint32_t target = (uint32_t)(((size_t)z * H + y) * W + x);
+    const uint32_t target = (uint32_t)((z * H + y) * W + x);
     const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
     const uint32_t old = win[wc];
     const uint32_t nw = win[wc + S.woff[pick]];
@@ -295,26 +371,15 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
     }
 
     if (old != 0) {
-        // The per-colour guard: the losing cell must keep a site of another
-        // colour. A like neighbour is one, since every neighbour of a target
-        // is of another colour.
-        if (like_old == 0) {
-            int other = 0;
-            for (int c = 0; c < a.g.ncol; ++c)
-                if (c != a.colour) other += a.vol_by_colour[(size_t)old * a.g.ncol + c];
-            if (other == 0) return;
-        }
-        if (a.g.ring_n > 0 && a.t.connected[t_old]) {
-            uint32_t present = 0;
-            for (int k = 0; k < a.g.ring_n; ++k)
-                if (win[wc + S.wring[k]] == old) present |= 1u << k;
-            if (!one_piece(present, a.g.adjacency)) return;
-        }
+        // A like neighbour is a site of another colour, since every neighbour
+        // of a target is; only a target with none needs the per-colour count.
+        if (like_old == 0 && !keeps_other_colour(a, old)) return;
+        if (a.g.ring_n > 0 && a.t.connected[t_old] && !ring_one_piece(a, S.wring, win, wc, old)) return;
     }
     const int ds_old = 2 * like_old - NOFF;
     const int ds_new = NOFF - 2 * like_new;
 
-    int vol_old = 0, surf_old = 0, vol_new = 0, surf_new = 0;
+    int vol_old, surf_old, vol_new, surf_new;
     {
         int dv, ds;
         unpack_delta(prev_old, dv, ds);
@@ -356,35 +421,8 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
         }
     }
-
-    long long terms_old[NM], terms_new[NM];
-    if (a.tracks) {
-        if (old != 0) {
-            const int *an = &a.anchor[(size_t)old * 4];
-            site_terms<DIM>(fold_int(x - an[0], W), fold_int(y - an[1], H), fold_int(z - an[2], D), terms_old);
-        }
-        if (nw != 0) {
-            const int *an = &a.anchor[(size_t)nw * 4];
-            site_terms<DIM>(fold_int(x - an[0], W), fold_int(y - an[1], H), fold_int(z - an[2], D), terms_new);
-        }
-        if (a.has_length) {
-            if (old != 0 && a.t.lambda_length[t_old] != 0.0)
-                delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_old, old, vol_old, terms_old, -1));
-            if (nw != 0 && a.t.lambda_length[t_new] != 0.0)
-                delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_new, nw, vol_new, terms_new, 1));
-        }
-    }
-
-    if (a.has_chemotaxis && nw != 0) {
-        const int ox = a.g.off[pick][0], oy = a.g.off[pick][1], oz = a.g.off[pick][2];
-        const uint32_t source = (uint32_t)(((size_t)wrap(z + oz, D) * H + wrap(y + oy, H)) * W + wrap(x + ox, W));
-        for (int s = 0; s < a.n_species; ++s) {
-            const float lam = a.t.chemotaxis[t_new * a.n_species + s];
-            if (lam == 0.0f) continue;
-            const float *f = a.fields[s];
-            delta = __fsub_rn(delta, __fmul_rn(lam, __fsub_rn(f[target], f[source])));
-        }
-    }
+    if (a.has_length || a.has_chemotaxis)
+        delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
 
     if (delta > 0.0f) {
         const float u = to_f32(draw(a.key_accept, target));
@@ -395,18 +433,12 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
     if (old != 0) {
         atomicAdd(&a.vs_cur[old], pack_delta(-1, ds_old));
         atomicSub(&a.vol_by_colour[(size_t)old * a.g.ncol + a.colour], 1);
-        if (a.tracks)
-#pragma unroll
-            for (int k = 0; k < NM; ++k)
-                atomicAdd(&a.mom_cur[(size_t)old * NM + k], (unsigned long long)(-terms_old[k]));
     }
     if (nw != 0) {
         atomicAdd(&a.vs_cur[nw], pack_delta(1, ds_new));
         atomicAdd(&a.vol_by_colour[(size_t)nw * a.g.ncol + a.colour], 1);
-        if (a.tracks)
-#pragma unroll
-            for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)nw * NM + k], (unsigned long long)terms_new[k]);
     }
+    if (a.tracks) commit_moments<DIM>(a, old, nw, x, y, z);
 }
 
 template <int DIM>
@@ -586,28 +618,38 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
         }
 
         // Light pass: every target's pick; only targets whose neighbour
-        // carries another label go into the tile's queue.
+        // carries another label go into the tile's queue. A warp keeps its
+        // entries in registers and reserves queue room once per tile.
         constexpr int PER_LANE = Smem::TPW / 32;
+        const bool full = x0 + T::TX <= W && y0 + T::TY <= H && (DIM == 2 || z0 + T::TZ <= D);
+        const int tile_base = (z0 * H + y0) * W + x0;
+        uint32_t entries[PER_LANE];
+        unsigned masks[PER_LANE];
+        int total = 0;
 #pragma unroll
         for (int k = 0; k < PER_LANE; ++k) {
             const int j = warp * Smem::TPW + k * 32 + lane;
             int lx, ly, lz;
             target_of<DIM>(j, a.colour, lx, ly, lz);
-            const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
             bool active = false;
-            uint32_t entry = 0;
-            if (x < W && y < H && (DIM == 2 || z < D)) {
-                const uint32_t target = (uint32_t)(((size_t)z * H + y) * W + x);
+            if (full || (x0 + lx < W && y0 + ly < H && (DIM == 2 || z0 + lz < D))) {
+                const uint32_t target = (uint32_t)(tile_base + (lz * H + ly) * W + lx);
                 const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
                 const int pick = (int)(draw(a.key_pick, target) % (uint64_t)NOFF);
                 active = win[wc] != win[wc + S.woff[pick]];
-                entry = (uint32_t)j | ((uint32_t)pick << 16);
+                entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
             }
-            const unsigned mask = __ballot_sync(0xffffffffu, active);
-            int base = 0;
-            if (lane == 0 && mask) base = atomicAdd(&S.queued, __popc(mask));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (active) S.queue[base + __popc(mask & ((1u << lane) - 1u))] = entry;
+            masks[k] = __ballot_sync(0xffffffffu, active);
+            total += __popc(masks[k]);
+        }
+        int base = 0;
+        if (lane == 0 && total) base = atomicAdd(&S.queued, total);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+        for (int k = 0; k < PER_LANE; ++k) {
+            if (masks[k] & (1u << lane)) S.queue[base + __popc(masks[k] & below)] = entries[k];
+            base += __popc(masks[k]);
         }
         __syncthreads();
         // Heavy pass: warps take the queue 32 copies at a time.
