@@ -136,6 +136,9 @@ def lib():
     L.glz_gpu_set_labels.argtypes = [_P, _P, C.c_size_t]
     L.glz_gpu_step_profiled.restype = C.c_int
     L.glz_gpu_step_profiled.argtypes = [_P, C.c_uint64, C.POINTER(C.c_double)]
+    L.glz_field_step_noalloc.restype = C.c_int
+    L.glz_field_step_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P,
+                                         C.c_size_t, _P, _P, _P]
     L.glz_gpu_destroy.restype = None
     L.glz_gpu_destroy.argtypes = [_P]
     _declare_extras(L)

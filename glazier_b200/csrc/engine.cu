@@ -26,8 +26,14 @@ int sweep_box(int dim, uint32_t box[3]);
 }
 
 namespace {
-
 thread_local std::string g_error = "no error";
+}
+
+namespace glz {
+void set_last_error(const std::string &msg) { g_error = msg; }
+}
+
+namespace {
 
 int fail(int code, const std::string &msg) {
     g_error = msg;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 
 namespace glz {
 
@@ -148,6 +149,9 @@ struct PopulationLaunch {
     uint32_t *daughter;
     int *counters;           // [0] daughters issued, [1] events
 };
+
+// Record the message glz_last_error() returns on this thread.
+void set_last_error(const std::string &msg);
 
 cudaError_t launch_population_plan(const PopulationLaunch &a, cudaStream_t stream);
 cudaError_t launch_population_apply(const PopulationLaunch &a, cudaStream_t stream);

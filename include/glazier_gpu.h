@@ -148,6 +148,44 @@ int glz_gpu_device_field(glz_gpu *h, int index, void **field);
 /* Release the device state: Drop for GpuSimulation. NULL is a no-op. */
 void glz_gpu_destroy(glz_gpu *h);
 
+/* The most f32 values of intermediate fields glz_field_step_noalloc holds:
+ * 4,194,304 (16 MiB), beside a table area of 1,024 values. */
+#define GLZ_NOALLOC_FIELD_SCRATCH (1u << 22)
+
+/*
+ * One Monte Carlo step of the chemical-field solver on buffers the caller
+ * owns, allocating nothing. No counterpart in the reference: it serves callers
+ * that cannot call cudaMalloc, such as a host application that fixes its
+ * device-memory budget at start-up and forbids allocation afterwards, or a
+ * coupled solver that hands this library only buffers it owns.
+ *
+ * The arithmetic is the engine's own field step (glz_gpu_step's): per species
+ * ceil(D / (1/(2 dim))) sub-steps of FTCS diffusion and decay, secretion and
+ * uptake by each site's owner folded into the species' last sub-step.
+ *   width, height, depth   the lattice; n_species 1..8, n_types 1..64
+ *   diffusion, decay       host, n_species values each
+ *   secretion, uptake      host, n_types * n_species values, [type][species]
+ *   labels, cell_type      device: one label per site; n_labels types
+ *   fields_in, fields_out  device, n_species * sites f32, species-major;
+ *                          distinct buffers
+ *   stream                 a cudaStream_t, or NULL for the default stream
+ * The work is queued on `stream`; the call does not wait for it.
+ *
+ * The scratch (the per-type tables and up to GLZ_NOALLOC_FIELD_SCRATCH
+ * values of intermediate fields: none for one sub-step, one buffer per
+ * species for two, two for three or more) lives in one fixed array in device
+ * memory that every GPU loading this library holds until the process exits. A
+ * step needing more is refused with GLZ_INVALID. The first call on a device
+ * looks up that array's device address; make it before any stream capture.
+ * Every call shares the array and nothing in it needs to start at zero, but
+ * two calls whose work overlaps on the GPU race on it: order them on one
+ * stream or wait between them.
+ */
+int glz_field_step_noalloc(int width, int height, int depth, int n_species, int n_types, const double *diffusion,
+                           const double *decay, const double *secretion, const double *uptake,
+                           const uint32_t *labels, const uint8_t *cell_type, size_t n_labels,
+                           const float *fields_in, float *fields_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
