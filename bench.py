@@ -148,6 +148,44 @@ def committed_traffic():
     return None
 
 
+def ensemble_compare(mcs: int, device: int) -> dict:
+    """64 uneven monolayer replicas (sides log-uniform 128..1024, own T, J and
+    lambda_V): one batched ensemble under a CUDA graph against looping the
+    plain engine over the same replicas. Both wait for their own results; the
+    replicas' lattices come out identical."""
+    import torch
+
+    from glazier_b200.engine import GpuSimulation
+    from glazier_b200.ensemble import Ensemble
+    from glazier_b200.workloads import ensemble_starts
+
+    starts = ensemble_starts(64)
+    sites = sum(st.model.sites for st in starts)
+    ens = Ensemble(starts, device=device)
+    choice = ens.autotune(3)
+    ens.step(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    device_ms = ens.step_timed(mcs)
+    batched_s = time.perf_counter() - t0
+    sims = [GpuSimulation.from_start(st, device=device) for st in starts]
+    for sim in sims:
+        sim.step(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sim in sims:
+        sim.step(mcs)
+    looped_s = time.perf_counter() - t0
+    same = all(np.array_equal(ens.labels(i), sims[i].labels()) for i in (0, 17, 63))
+    for sim in sims:
+        sim.close()
+    ens.close()
+    return {"replicas": 64, "sites": sites, "mcs": mcs, "batched_s": batched_s, "batched_device_ms": device_ms,
+            "looped_plain_s": looped_s, "speedup": looped_s / batched_s,
+            "batched_site_updates_per_s": sites * mcs / batched_s, "schedule_choice": choice,
+            "lattices_identical": bool(same)}
+
+
 def cpu_baseline(size: int, seconds: float) -> dict:
     """The serial engine on one host core, a bounded sample of the same lattice."""
     from oracle.serial import SerialOracle
@@ -319,6 +357,8 @@ def run_ours(args) -> None:
         "clocks": clocks.summary(),
         "phase_ms": {"sweep": sweep_ms, "fields": field_ms, "population": pop_ms},
     }
+    if world == 1 and not args.no_ensemble:
+        line["ensemble"] = ensemble_compare(100, torch.cuda.current_device())
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, args.cpu_seconds)
     print(json.dumps(line), flush=True)
@@ -334,6 +374,7 @@ def main() -> None:
     ap.add_argument("--e2e-jobs", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

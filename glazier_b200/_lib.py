@@ -147,8 +147,30 @@ def lib():
 
 
 def _declare_extras(L) -> None:
-    """Signatures of the optional entry points, declared where present."""
-    return None
+    """Signatures of the batched ensemble's entry points."""
+    L.glz_ens_create.restype = C.c_int
+    L.glz_ens_create.argtypes = [C.c_int, C.POINTER(GlzModel), C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_size_t),
+                                 C.POINTER(_P)]
+    L.glz_ens_step.restype = C.c_int
+    L.glz_ens_step.argtypes = [_P, C.c_uint64]
+    L.glz_ens_step_timed.restype = C.c_int
+    L.glz_ens_step_timed.argtypes = [_P, C.c_uint64, C.POINTER(C.c_double)]
+    L.glz_ens_autotune.restype = C.c_int
+    L.glz_ens_autotune.argtypes = [_P, C.c_uint64, C.POINTER(C.c_int)]
+    L.glz_ens_set_schedule.restype = C.c_int
+    L.glz_ens_set_schedule.argtypes = [_P, C.c_int, C.c_int]
+    L.glz_ens_labels.restype = C.c_int
+    L.glz_ens_labels.argtypes = [_P, C.c_int, _P, C.c_size_t]
+    L.glz_ens_volumes.restype = C.c_int
+    L.glz_ens_volumes.argtypes = [_P, C.c_int, _P, C.POINTER(C.c_size_t)]
+    L.glz_ens_surfaces.restype = C.c_int
+    L.glz_ens_surfaces.argtypes = [_P, C.c_int, _P, C.POINTER(C.c_size_t)]
+    L.glz_ens_mcs.restype = C.c_uint64
+    L.glz_ens_mcs.argtypes = [_P]
+    L.glz_ens_stream.restype = _P
+    L.glz_ens_stream.argtypes = [_P]
+    L.glz_ens_destroy.restype = None
+    L.glz_ens_destroy.argtypes = [_P]
 
 
 def last_error() -> str:

@@ -87,6 +87,44 @@ struct SweepLaunch {
 
 cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream);
 
+// The batched ensemble: independent replicas of one neighbourhood, all their
+// tiles in one persistent launch per colour. Replica state lives in flat
+// arrays; each replica's SweepLaunch holds its static fields (geometry,
+// tables, absolute label/type/colour-count pointers) and the kernel patches
+// the per-pass ones from the clock.
+struct EnsembleClock {
+    long long step;  // Monte Carlo steps completed
+    long long pass;  // colour passes completed
+};
+
+struct EnsembleReplica {
+    SweepLaunch a;
+    long long cell_off;  // first entry of this replica in the flat per-cell arrays
+    uint64_t seed;
+};
+
+struct EnsembleLaunch {
+    int n;             // replicas
+    int total_tiles;
+    int colour;
+    int max_ctas;
+    const EnsembleReplica *replicas;
+    const void *maps;        // one CUtensorMap per replica (64-byte aligned), or null
+    const int *tile_prefix;  // n + 1 entries, in schedule order
+    const int *order;        // schedule position -> replica
+    const EnsembleClock *clock;
+    int2 *vs_base[2];
+    long long *vs_delta[3];
+    long long total_cells;
+    int ncol;
+    int uniform_contact_exact;
+    int *error_flag;
+};
+
+cudaError_t launch_ensemble_sweep(const EnsembleLaunch &e, int dim, int n_off, bool uniform, cudaStream_t stream);
+cudaError_t launch_clock_advance(EnsembleClock *clock, int ncol, cudaStream_t stream);
+int ensemble_grid_cap(int dim, int n_off, bool uniform);
+
 struct FieldLaunch {
     Geometry g;
     int n_species;

@@ -485,6 +485,100 @@ __device__ __forceinline__ void issue_window(const CUtensorMap &tmap, uint32_t *
     }
 }
 
+// Wrapped plain loads of a tile's window, for tiles on the periodic edge and
+// lattices whose rows are not whole 16-byte units.
+template <int DIM>
+__device__ __forceinline__ void load_window_plain(const SweepLaunch &a, uint32_t *win, int x0, int y0, int z0) {
+    using T = Tile<DIM>;
+    using Smem = SweepSmem<DIM>;
+    const int tid = threadIdx.x;
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    // A lattice at least a window wide wraps each coordinate at most
+    // once, by a compare; a smaller one takes the remainder.
+    const bool once = W >= T::PX && H >= T::PY && (DIM == 2 || D >= T::PZ);
+    for (int i = tid; i < Smem::WIN; i += blockDim.x) {
+        const int px = i % T::PX;
+        const int py = (i / T::PX) % T::PY;
+        const int pz = i / (T::PX * T::PY);
+        int gx = x0 - T::HX + px, gy = y0 - 1 + py, gz = DIM == 3 ? z0 - 1 + pz : 0;
+        if (once) {
+            gx += gx < 0 ? W : (gx >= W ? -W : 0);
+            gy += gy < 0 ? H : (gy >= H ? -H : 0);
+            if (DIM == 3) gz += gz < 0 ? D : (gz >= D ? -D : 0);
+        } else {
+            gx = wrap(gx, W);
+            gy = wrap(gy, H);
+            gz = DIM == 3 ? wrap(gz, D) : 0;
+        }
+        win[i] = a.labels[((size_t)gz * H + gy) * W + gx];
+    }
+    // generic writes to a buffer a later tensor copy will overwrite
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+}
+
+// Price every target of the pass's colour in one tile whose window is in
+// shared memory: the light pass queues the targets whose neighbour pick
+// carries another label, the heavy pass prices and commits the queue.
+template <int DIM, int NOFF, bool UNIFORM>
+__device__ __forceinline__ void price_tile(const SweepLaunch &a, SweepSmem<DIM> &S, const uint32_t *win, int x0,
+                                           int y0, int z0, bool small_types) {
+    using T = Tile<DIM>;
+    using Smem = SweepSmem<DIM>;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    // Light pass: every target's pick; only targets whose neighbour
+    // carries another label go into the tile's queue. A warp keeps its
+    // entries in registers and reserves queue room once per tile.
+    constexpr int PER_LANE = Smem::TPW / 32;
+    const bool full = x0 + T::TX <= W && y0 + T::TY <= H && (DIM == 2 || z0 + T::TZ <= D);
+    const int tile_base = (z0 * H + y0) * W + x0;
+    uint32_t entries[PER_LANE];
+    unsigned masks[PER_LANE];
+    int total = 0;
+#pragma unroll
+    for (int k = 0; k < PER_LANE; ++k) {
+        const int j = warp * Smem::TPW + k * 32 + lane;
+        int lx, ly, lz;
+        target_of<DIM>(j, a.colour, lx, ly, lz);
+        bool active = false;
+        if (full || (x0 + lx < W && y0 + ly < H && (DIM == 2 || z0 + lz < D))) {
+            const uint32_t target = (uint32_t)(tile_base + (lz * H + ly) * W + lx);
+            const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
+            const int pick = (int)(draw(a.key_pick, target) % (uint64_t)NOFF);
+            active = win[wc] != win[wc + S.woff[pick]];
+            entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
+        }
+        masks[k] = __ballot_sync(0xffffffffu, active);
+        total += __popc(masks[k]);
+    }
+    int base = 0;
+    if (lane == 0 && total) base = atomicAdd(&S.queued, total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < PER_LANE; ++k) {
+        if (masks[k] & (1u << lane)) S.queue[base + __popc(masks[k] & below)] = entries[k];
+        base += __popc(masks[k]);
+    }
+    __syncthreads();
+    // Heavy pass: warps take the queue 32 copies at a time.
+    const int queued = S.queued;
+    for (;;) {
+        int first = 0;
+        if (lane == 0) first = atomicAdd(&S.taken, 32);
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (first >= queued) break;
+        if (first + lane < queued)
+            price_and_commit<DIM, NOFF, UNIFORM>(a, S, win, S.queue[first + lane], x0, y0, z0, small_types);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        S.queued = 0;
+        S.taken = 0;
+    }
+}
+
 // Wait for phase `parity` of an mbarrier, giving up after kWaitLimit polls.
 __device__ __forceinline__ uint32_t wait_parity(unsigned long long *bar, uint32_t parity) {
     const uint32_t b = smem_addr(bar);
@@ -593,80 +687,9 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
                 return;
             }
         } else {
-            // A lattice at least a window wide wraps each coordinate at most
-            // once, by a compare; a smaller one takes the remainder.
-            const bool once = W >= T::PX && H >= T::PY && (DIM == 2 || D >= T::PZ);
-            for (int i = tid; i < Smem::WIN; i += blockDim.x) {
-                const int px = i % T::PX;
-                const int py = (i / T::PX) % T::PY;
-                const int pz = i / (T::PX * T::PY);
-                int gx = x0 - T::HX + px, gy = y0 - 1 + py, gz = DIM == 3 ? z0 - 1 + pz : 0;
-                if (once) {
-                    gx += gx < 0 ? W : (gx >= W ? -W : 0);
-                    gy += gy < 0 ? H : (gy >= H ? -H : 0);
-                    if (DIM == 3) gz += gz < 0 ? D : (gz >= D ? -D : 0);
-                } else {
-                    gx = wrap(gx, W);
-                    gy = wrap(gy, H);
-                    gz = DIM == 3 ? wrap(gz, D) : 0;
-                }
-                win[i] = a.labels[((size_t)gz * H + gy) * W + gx];
-            }
-            // generic writes to a buffer a later tensor copy will overwrite
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
+            load_window_plain<DIM>(a, win, x0, y0, z0);
         }
-
-        // Light pass: every target's pick; only targets whose neighbour
-        // carries another label go into the tile's queue. A warp keeps its
-        // entries in registers and reserves queue room once per tile.
-        constexpr int PER_LANE = Smem::TPW / 32;
-        const bool full = x0 + T::TX <= W && y0 + T::TY <= H && (DIM == 2 || z0 + T::TZ <= D);
-        const int tile_base = (z0 * H + y0) * W + x0;
-        uint32_t entries[PER_LANE];
-        unsigned masks[PER_LANE];
-        int total = 0;
-#pragma unroll
-        for (int k = 0; k < PER_LANE; ++k) {
-            const int j = warp * Smem::TPW + k * 32 + lane;
-            int lx, ly, lz;
-            target_of<DIM>(j, a.colour, lx, ly, lz);
-            bool active = false;
-            if (full || (x0 + lx < W && y0 + ly < H && (DIM == 2 || z0 + lz < D))) {
-                const uint32_t target = (uint32_t)(tile_base + (lz * H + ly) * W + lx);
-                const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
-                const int pick = (int)(draw(a.key_pick, target) % (uint64_t)NOFF);
-                active = win[wc] != win[wc + S.woff[pick]];
-                entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
-            }
-            masks[k] = __ballot_sync(0xffffffffu, active);
-            total += __popc(masks[k]);
-        }
-        int base = 0;
-        if (lane == 0 && total) base = atomicAdd(&S.queued, total);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        const unsigned below = (1u << lane) - 1u;
-#pragma unroll
-        for (int k = 0; k < PER_LANE; ++k) {
-            if (masks[k] & (1u << lane)) S.queue[base + __popc(masks[k] & below)] = entries[k];
-            base += __popc(masks[k]);
-        }
-        __syncthreads();
-        // Heavy pass: warps take the queue 32 copies at a time.
-        const int queued = S.queued;
-        for (;;) {
-            int first = 0;
-            if (lane == 0) first = atomicAdd(&S.taken, 32);
-            first = __shfl_sync(0xffffffffu, first, 0);
-            if (first >= queued) break;
-            if (first + lane < queued)
-                price_and_commit<DIM, NOFF, UNIFORM>(a, S, win, S.queue[first + lane], x0, y0, z0, small_types);
-        }
-        __syncthreads();
-        if (tid == 0) {
-            S.queued = 0;
-            S.taken = 0;
-        }
+        price_tile<DIM, NOFF, UNIFORM>(a, S, win, x0, y0, z0, small_types);
     }
 }
 
@@ -719,6 +742,213 @@ static cudaError_t launch_any(const SweepLaunch &a, cudaStream_t stream) {
 cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream) {
     return a.uniform_type >= 0 && a.uniform_contact_exact ? launch_any<true>(a, stream) : launch_any<false>(a, stream);
 }
+
+
+// ---------------------------------------------------------------- the ensemble
+
+template <int DIM>
+struct EnsembleSmem {
+    SweepSmem<DIM> s;
+    SweepLaunch desc;  // the current replica's launch, per-pass fields patched
+    int replica;       // the replica `desc` holds, -1 before the first tile
+    int next_replica;
+};
+
+// The schedule position of tile t: the last prefix entry at or below it.
+__device__ __forceinline__ int replica_of_tile(const int *prefix, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+__global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
+    ensemble_sweep_kernel(const __grid_constant__ EnsembleLaunch e) {
+    using T = Tile<DIM>;
+    using Smem = SweepSmem<DIM>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    EnsembleSmem<DIM> &E = *reinterpret_cast<EnsembleSmem<DIM> *>(smem_raw + ((128u - (raw & 127u)) & 127u));
+    Smem &S = E.s;
+    const int tid = threadIdx.x;
+    if (smem_addr(S.win[0]) & 127u) {
+        if (tid == 0) atomicExch(e.error_flag, 3);
+        return;
+    }
+    const long long step = e.clock->step;
+    const long long pass = e.clock->pass + e.colour;
+
+    // Tally rotation for the next pass over every replica's cells at once.
+    {
+        const size_t stride = (size_t)gridDim.x * blockDim.x;
+        int2 *const base = e.vs_base[pass % 2];
+        const long long *const prev = e.vs_delta[(pass + 2) % 3];
+        int2 *const next_base = e.vs_base[(pass + 1) % 2];
+        long long *const clear = e.vs_delta[(pass + 1) % 3];
+        for (size_t l = (size_t)blockIdx.x * blockDim.x + tid; l < (size_t)e.total_cells; l += stride) {
+            int dv, ds;
+            unpack_delta(prev[l], dv, ds);
+            const int2 b = base[l];
+            next_base[l] = make_int2(b.x + dv, b.y + ds);
+            clear[l] = 0;
+        }
+    }
+    if (tid < NOFF) S.woff[tid] = window_offset<DIM, NOFF>(tid);
+    if (tid == 0) {
+        S.queued = 0;
+        S.taken = 0;
+        E.replica = -1;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const CUtensorMap *maps = static_cast<const CUtensorMap *>(e.maps);
+    int waited[2] = {0, 0};
+    bool pending[2] = {false, false};
+    // The position, origin and tensor-copy eligibility of global tile t.
+    auto locate = [&](int t, int &pos, int &x0, int &y0, int &z0) -> bool {
+        pos = replica_of_tile(e.tile_prefix, e.n, t);
+        const SweepLaunch &ra = e.replicas[e.order[pos]].a;
+        tile_origin<DIM>(t - e.tile_prefix[pos], ra.g.w, ra.g.h, x0, y0, z0);
+        return maps != nullptr && tile_interior<DIM>(ra, x0, y0, z0);
+    };
+    int t = blockIdx.x;
+    if (t < e.total_tiles) {
+        int pos, x0, y0, z0;
+        if (locate(t, pos, x0, y0, z0)) {
+            if (tid == 0) issue_window<DIM>(maps[e.order[pos]], S.win[0], &S.mbar[0], x0, y0, z0);
+            pending[0] = true;
+        }
+    }
+    for (int it = 0; t < e.total_tiles; t += gridDim.x, ++it) {
+        const int buf = it & 1;
+        int pos, x0, y0, z0;
+        const bool interior = locate(t, pos, x0, y0, z0);
+        const int r = e.order[pos];
+        const int next = t + gridDim.x;
+        if (next < e.total_tiles) {
+            int npos, nx0, ny0, nz0;
+            if (locate(next, npos, nx0, ny0, nz0)) {
+                if (tid == 0) issue_window<DIM>(maps[e.order[npos]], S.win[buf ^ 1], &S.mbar[buf ^ 1], nx0, ny0, nz0);
+                pending[buf ^ 1] = true;
+            }
+        }
+        if (r != E.replica) {
+            // Bring this replica's launch into shared memory and patch the
+            // per-pass fields: keys, tally rotation, colour, step.
+            __syncthreads();
+            const EnsembleReplica &rep = e.replicas[r];
+            const int *src = reinterpret_cast<const int *>(&rep.a);
+            int *dst = reinterpret_cast<int *>(&E.desc);
+            for (int i = tid; i < (int)(sizeof(SweepLaunch) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+            __syncthreads();
+            if (tid == 0) {
+                SweepLaunch &d = E.desc;
+                d.colour = e.colour;
+                d.step = (int32_t)step;
+                d.key_pick = stream_key(rep.seed, d.step, e.colour, 0);
+                d.key_accept = stream_key(rep.seed, d.step, e.colour, 1);
+                d.vs_base = e.vs_base[pass % 2] + rep.cell_off;
+                d.vs_prev = e.vs_delta[(pass + 2) % 3] + rep.cell_off;
+                d.vs_cur = reinterpret_cast<unsigned long long *>(e.vs_delta[pass % 3] + rep.cell_off);
+                E.replica = r;
+            }
+            const bool small = rep.a.n_types <= kSmemTypes;
+            if (small)
+                for (int i = tid; i < rep.a.n_types * rep.a.n_types; i += blockDim.x) S.contact[i] = rep.a.t.contact[i];
+            __syncthreads();
+        }
+        const SweepLaunch &a = E.desc;
+        uint32_t *win = S.win[buf];
+        if (interior) {
+            const uint32_t done = wait_parity(&S.mbar[buf], waited[buf] & 1);
+            waited[buf] += 1;
+            pending[buf] = false;
+            if (!__syncthreads_and(done)) {
+                if (pending[buf ^ 1]) wait_parity(&S.mbar[buf ^ 1], waited[buf ^ 1] & 1);
+                if (tid == 0) atomicExch(e.error_flag, 1);
+                return;
+            }
+        } else {
+            load_window_plain<DIM>(a, win, x0, y0, z0);
+        }
+        price_tile<DIM, NOFF, UNIFORM>(a, S, win, x0, y0, z0, a.n_types <= kSmemTypes);
+    }
+}
+
+__global__ void clock_advance_kernel(EnsembleClock *clock, int ncol) {
+    clock->step += 1;
+    clock->pass += ncol;
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+static int ensemble_cap() {
+    static int cap = 0;
+    if (!cap) {
+        const size_t smem = sizeof(EnsembleSmem<DIM>) + 128;
+        if (cudaFuncSetAttribute(ensemble_sweep_kernel<DIM, NOFF, UNIFORM>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))
+            return 0;
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_sweep_kernel<DIM, NOFF, UNIFORM>, kThreads,
+                                                          smem))
+            return 0;
+        cap = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    return cap;
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+static cudaError_t ensemble_launch(const EnsembleLaunch &e, cudaStream_t stream) {
+    const int cap = ensemble_cap<DIM, NOFF, UNIFORM>();
+    if (!cap) return cudaErrorInvalidConfiguration;
+    int grid = e.total_tiles < cap ? e.total_tiles : cap;
+    if (e.max_ctas > 0 && grid > e.max_ctas) grid = e.max_ctas;
+    const size_t smem = sizeof(EnsembleSmem<DIM>) + 128;
+    ensemble_sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kThreads, smem, stream>>>(e);
+    return cudaGetLastError();
+}
+
+template <bool UNIFORM>
+static cudaError_t ensemble_any(const EnsembleLaunch &e, int dim, int n_off, cudaStream_t stream) {
+    if (dim == 2) {
+        if (n_off == 4) return ensemble_launch<2, 4, UNIFORM>(e, stream);
+        if (n_off == 8) return ensemble_launch<2, 8, UNIFORM>(e, stream);
+    } else {
+        if (n_off == 6) return ensemble_launch<3, 6, UNIFORM>(e, stream);
+        if (n_off == 18) return ensemble_launch<3, 18, UNIFORM>(e, stream);
+        if (n_off == 26) return ensemble_launch<3, 26, UNIFORM>(e, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_ensemble_sweep(const EnsembleLaunch &e, int dim, int n_off, bool uniform, cudaStream_t stream) {
+    return uniform ? ensemble_any<true>(e, dim, n_off, stream) : ensemble_any<false>(e, dim, n_off, stream);
+}
+
+cudaError_t launch_clock_advance(EnsembleClock *clock, int ncol, cudaStream_t stream) {
+    clock_advance_kernel<<<1, 1, 0, stream>>>(clock, ncol);
+    return cudaGetLastError();
+}
+
+template <bool UNIFORM>
+static int cap_any(int dim, int n_off) {
+    if (dim == 2) return n_off == 4 ? ensemble_cap<2, 4, UNIFORM>() : ensemble_cap<2, 8, UNIFORM>();
+    if (n_off == 6) return ensemble_cap<3, 6, UNIFORM>();
+    if (n_off == 18) return ensemble_cap<3, 18, UNIFORM>();
+    return ensemble_cap<3, 26, UNIFORM>();
+}
+
+int ensemble_grid_cap(int dim, int n_off, bool uniform) { return uniform ? cap_any<true>(dim, n_off) : cap_any<false>(dim, n_off); }
 
 // The box a sweep tile's tensor copy moves: the tile plus its halo.
 int sweep_box(int dim, uint32_t box[3]) {

@@ -1,0 +1,92 @@
+"""Synthetic starts with the shapes of the scaling, ensemble and field runs.
+
+No public dataset is involved: every start is a tiling of square (or cubic)
+cells, built the way the reference's own benchmark builds its lattices
+(glazier/examples/bench.rs, Lattice::tile_grid in lattice.rs:169-196), with
+parameters drawn from a counter hash of (seed, index) so a run is the same on
+every machine.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .blueprint import CellType, Model, Start
+
+_M64 = (1 << 64) - 1
+
+
+def _mix(z: int) -> int:
+    """SplitMix64's finaliser, the mixer of the engine's counter hash."""
+    z = (z + 0x9E3779B97F4A7C15) & _M64
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return z ^ (z >> 31)
+
+
+def uniform01(seed: int, index: int, draw: int) -> float:
+    """A float in [0, 1) from (seed, index, draw), top 53 bits."""
+    return (_mix(seed ^ ((index * 0xD1B54A32D192ED03) & _M64) ^ ((draw * 0xA0761D6478BD642F) & _M64)) >> 11) / 2.0**53
+
+
+def monolayer(size: int, depth: int = 1, contact: float = 10.0, lambda_volume: float = 1.0,
+              target_volume: float | None = None, lambda_surface: float = 0.0, target_surface: float = 0.0,
+              temperature: float = 10.0, seed: int = 1, side: int = 8, order: int | None = None) -> Start:
+    """A periodic lattice tiled by cubes (squares in a plane) of `side`, one
+    cell type, no medium: the plain monolayer and its scaling sweep."""
+    if target_volume is None:
+        target_volume = float(side**2 if depth == 1 else side**3)
+    model = Model(
+        width=size,
+        height=size,
+        depth=depth,
+        contact=[0.0, contact, contact, contact],
+        types=[CellType(), CellType(target_volume=target_volume, lambda_volume=lambda_volume,
+                                    target_surface=target_surface, lambda_surface=lambda_surface)],
+        temperature=temperature,
+        neighbour_order=order if order is not None else (2 if depth == 1 else 3),
+        seed=seed,
+    )
+    return Start.tiled(model, side)
+
+
+def initial_surface(side: int, depth: int = 1) -> float:
+    """Unlike-bond count of one isolated square (cube) of `side` under the
+    Moore (26) neighbourhood: what a tiled cell starts with."""
+    if depth == 1:
+        edge = 4 * (side - 2)
+        return float(4 * 5 + edge * 3)
+    # a cube: count neighbours outside for every boundary site
+    n = 0
+    rng = range(side)
+    for z in rng:
+        for y in rng:
+            for x in rng:
+                for dz in (-1, 0, 1):
+                    for dy in (-1, 0, 1):
+                        for dx in (-1, 0, 1):
+                            if (dx, dy, dz) == (0, 0, 0):
+                                continue
+                            if not (0 <= x + dx < side and 0 <= y + dy < side and 0 <= z + dz < side):
+                                n += 1
+    return float(n)
+
+
+def ensemble_starts(count: int = 64, seed: int = 1, side: int = 8, low: int = 128, high: int = 1024) -> list:
+    """`count` monolayer replicas with lattice sides log-uniform from `low` to
+    `high` (rounded to whole cells), temperature uniform in [5, 20], contact
+    energy uniform in [6, 16] on a 1/64 grid, volume constraint uniform in
+    [0.5, 2], each with its own seed."""
+    starts = []
+    for i in range(count):
+        u = [uniform01(seed, i, k) for k in range(4)]
+        size = side * round(2 ** (math.log2(low) + u[0] * (math.log2(high) - math.log2(low))) / side)
+        size += size % 2
+        temperature = 5.0 + 15.0 * u[1]
+        contact = 6.0 + round(10.0 * u[2] * 64) / 64
+        lambda_volume = 0.5 + 1.5 * u[3]
+        starts.append(monolayer(size, contact=contact, lambda_volume=lambda_volume, temperature=temperature,
+                                seed=(seed * 1_000_003 + i) & _M64, side=side))
+    return starts

@@ -148,6 +148,40 @@ int glz_gpu_device_field(glz_gpu *h, int index, void **field);
 /* Release the device state: Drop for GpuSimulation. NULL is a no-op. */
 void glz_gpu_destroy(glz_gpu *h);
 
+/* ---------------------------------------------------------------- ensemble
+ *
+ * A batch of independent replicas run as one: every replica's tiles in one
+ * persistent launch per colour, one Monte Carlo step replayed from a CUDA
+ * graph. No reference counterpart (glazier runs one lattice per
+ * GpuSimulation); each replica's results are bit-identical to a glz_gpu_*
+ * run of the same start. Replicas may differ in size, parameters and seed but
+ * share one neighbourhood; the ensemble runs the contact, volume and surface
+ * terms and refuses models with fields, length, connectivity, population,
+ * motility, drift or nematic terms (GLZ_UNSUPPORTED).
+ */
+typedef struct glz_ens glz_ens;
+
+/* n replicas: models[i], labels[i] (sites_i labels), cell_types[i]
+ * (n_labels[i] types). */
+int glz_ens_create(int n, const glz_model *models, const uint32_t *const *labels, const uint8_t *const *cell_types,
+                   const size_t *n_labels, glz_ens **out);
+/* Run `steps` Monte Carlo steps of every replica and wait. */
+int glz_ens_step(glz_ens *h, uint64_t steps);
+/* The same, reporting the device milliseconds the steps took. */
+int glz_ens_step_timed(glz_ens *h, uint64_t steps, double *ms);
+/* Time each schedule (replica order x persistent grid) on a snapshot of the
+ * state for `trial_steps` steps, restore the state, keep the fastest. */
+int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice);
+/* Choose a schedule directly: 0 replicas in order, 1 largest first;
+ * max_ctas 0 for one full wave. Results do not depend on it. */
+int glz_ens_set_schedule(glz_ens *h, int schedule, int max_ctas);
+int glz_ens_labels(glz_ens *h, int replica, uint32_t *out, size_t sites);
+int glz_ens_volumes(glz_ens *h, int replica, uint32_t *out, size_t *count);
+int glz_ens_surfaces(glz_ens *h, int replica, int64_t *out, size_t *count);
+uint64_t glz_ens_mcs(const glz_ens *h);
+void *glz_ens_stream(glz_ens *h);
+void glz_ens_destroy(glz_ens *h);
+
 /* The most f32 values of intermediate fields glz_field_step_noalloc holds:
  * 4,194,304 (16 MiB), beside a table area of 1,024 values. */
 #define GLZ_NOALLOC_FIELD_SCRATCH (1u << 22)

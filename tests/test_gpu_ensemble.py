@@ -1,0 +1,112 @@
+"""The batched ensemble against the plain engine, replica by replica.
+
+Every replica of an ensemble must land on exactly the lattice, volumes and
+surfaces a GpuSimulation of the same start lands on, whatever schedule the
+ensemble runs (replica order, persistent grid, tensor-copy windows on or off)
+and after the autotuner has timed its candidates on a snapshot.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from glazier_b200.blueprint import Start
+from glazier_b200.workloads import ensemble_starts, monolayer
+from oracle.replay import ReplayOracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _starts():
+    # uneven sides and rectangles, each with its own parameters and seed
+    out = []
+    for i, (w, h) in enumerate([(64, 64), (160, 96), (128, 128), (96, 200), (288, 64), (72, 80)]):
+        st = monolayer(8, contact=6.0 + i, lambda_volume=0.5 + 0.25 * i, temperature=6.0 + 2 * i, seed=100 + i,
+                       lambda_surface=0.1 * (i % 2), target_surface=92.0)
+        st.model.width, st.model.height = w, h
+        out.append(Start.tiled(st.model, 8))
+    return out
+
+
+def _plain(device, start, steps):
+    sim = device.GpuSimulation.from_start(start)
+    sim.step(steps)
+    return sim.labels(), sim.volumes(), sim.surfaces()
+
+
+@pytest.mark.parametrize("tma", ["1", "0"])
+def test_each_replica_matches_its_own_plain_run(device, tma, monkeypatch):
+    from glazier_b200.ensemble import Ensemble
+
+    monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
+    starts = _starts()
+    ens = Ensemble(starts)
+    ens.step(4)
+    ens.step(8)
+    assert ens.mcs == 12
+    for i, st in enumerate(starts):
+        labels, volumes, surfaces = _plain(device, st, 12)
+        assert np.array_equal(ens.labels(i), labels), f"replica {i}"
+        assert np.array_equal(ens.volumes(i), volumes), f"replica {i}"
+        assert np.array_equal(ens.surfaces(i), surfaces), f"replica {i}"
+    ens.close()
+
+
+def test_a_replica_matches_the_host_replay(device):
+    from glazier_b200.ensemble import Ensemble
+
+    starts = _starts()
+    ens = Ensemble(starts)
+    ens.step(6)
+    replay = ReplayOracle.from_start(starts[1])
+    replay.step(6)
+    assert np.array_equal(ens.labels(1), replay.labels())
+    assert np.array_equal(ens.volumes(1), replay.volumes())
+
+
+@pytest.mark.parametrize("schedule,ctas", [(0, 0), (1, 0), (0, 3), (1, 7)])
+def test_the_schedule_changes_only_the_time(device, schedule, ctas):
+    from glazier_b200.ensemble import Ensemble
+
+    starts = _starts()
+    ref = Ensemble(starts)
+    ref.step(5)
+    ens = Ensemble(starts)
+    ens.set_schedule(schedule, ctas)
+    ens.step(5)
+    for i in range(len(starts)):
+        assert np.array_equal(ens.labels(i), ref.labels(i)), f"replica {i}"
+
+
+def test_autotuning_leaves_the_run_where_it_was(device):
+    from glazier_b200.ensemble import Ensemble
+
+    starts = ensemble_starts(12, low=64, high=256)
+    ref = Ensemble(starts)
+    ref.step(3)
+    ens = Ensemble(starts)
+    ens.step(1)
+    choice = ens.autotune(2)
+    assert choice >= 0
+    assert ens.mcs == 1
+    ens.step(2)
+    for i in range(len(starts)):
+        assert np.array_equal(ens.labels(i), ref.labels(i)), f"replica {i}"
+        assert np.array_equal(ens.volumes(i), ref.volumes(i)), f"replica {i}"
+
+
+def test_the_ensemble_refuses_what_it_does_not_run(device):
+    from glazier_b200.engine import GpuError
+    from glazier_b200.ensemble import Ensemble
+
+    starts = _starts()[:2]
+    starts[1].model.types[1].division_volume = 100.0
+    with pytest.raises(GpuError, match="contact, volume and surface"):
+        Ensemble(starts)
+    odd = monolayer(64)
+    odd.model.width = 66
+    odd = Start.tiled(odd.model, 8)
+    odd.model.width = 65
+    with pytest.raises(GpuError):
+        Ensemble([odd])
