@@ -186,6 +186,60 @@ def ensemble_compare(mcs: int, device: int) -> dict:
             "lattices_identical": bool(same)}
 
 
+def adjoint_compare(steps: int, every: int, repeats: int, device: int) -> dict:
+    """The field adjoint at 512^2 (4096 cells, two fields, four types): record
+    `steps` MCS of owners from the engine, then time the adjoint's forward and
+    backward (checkpoint every `every` steps, with recompute) on its stream
+    with CUDA events, beside the plain engine's own field step over the same
+    steps. Algorithmic bytes: 20 per site per field per step."""
+    import torch
+
+    from glazier_b200.adjoint import FieldAdjoint, owner_types
+    from glazier_b200.engine import GpuSimulation
+    from glazier_b200.workloads import adjoint_start, uniform01
+
+    start = adjoint_start()
+    m = start.model
+    S, sites = len(m.species), m.sites
+    sim = GpuSimulation.from_start(start, device=device)
+    traj = np.empty((steps, sites), dtype=np.uint8)
+    field_ms = 0.0
+    for t in range(steps):
+        field_ms += sim.step_profiled(1)[1]
+        traj[t] = owner_types(sim.labels(), sim.cell_types())
+    sim.close()
+    params = np.concatenate([[sp.diffusion for sp in m.species], [sp.decay for sp in m.species],
+                             np.asarray(m.secretion, dtype=np.float64).reshape(-1),
+                             np.asarray(m.uptake, dtype=np.float64).reshape(-1)])
+    adj = FieldAdjoint(m.width, m.height, 1, S, m.n_types, traj, checkpoint_every=every, device=device)
+    f0 = torch.zeros(adj.shape, dtype=torch.float32, device=f"cuda:{device}")
+    noise = np.array([2.0 * uniform01(1, i, 9) - 1.0 for i in range(params.size)])
+    target = adj.forward(params * (1.0 + 0.1 * noise), f0)  # perturbed by 10% uniform noise
+    # the loss gradient at the final fields (the forward is deterministic)
+    grad = 2.0 * (adj.forward(params, f0) - target) / target.numel()
+    stream = torch.cuda.ExternalStream(adj.stream, device=f"cuda:{device}")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd, bwd = [], []
+    for r in range(repeats + 2):
+        ev[0].record(stream)
+        adj.forward(params, f0)
+        ev[1].record(stream)
+        adj.backward(grad)
+        ev[2].record(stream)
+        ev[2].synchronize()
+        if r >= 2:  # two warm-up rounds
+            fwd.append(ev[0].elapsed_time(ev[1]))
+            bwd.append(ev[1].elapsed_time(ev[2]))
+    adj.close()
+    f_ms, b_ms = statistics.median(fwd), statistics.median(bwd)
+    nbytes = 20 * sites * S * steps
+    return {"lattice": f"{m.width}x{m.height}", "cells": start.n_cells, "fields": S, "steps": steps,
+            "checkpoint_every": every, "forward_ms": f_ms, "backward_ms": b_ms,
+            "plain_field_step_ms": field_ms, "adjoint_over_plain": (f_ms + b_ms) / field_ms,
+            "achieved_gbs": nbytes / ((f_ms + b_ms) / 1e3) / 1e9, "bytes_per_site_field_step": 20,
+            "note": "fields are 1 MB each: the working set sits in L2, so HBM is not the bound here"}
+
+
 def cpu_baseline(size: int, seconds: float) -> dict:
     """The serial engine on one host core, a bounded sample of the same lattice."""
     from oracle.serial import SerialOracle
@@ -359,6 +413,8 @@ def run_ours(args) -> None:
     }
     if world == 1 and not args.no_ensemble:
         line["ensemble"] = ensemble_compare(100, torch.cuda.current_device())
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_compare(50, 10, 5, torch.cuda.current_device())
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, args.cpu_seconds)
     print(json.dumps(line), flush=True)
@@ -375,6 +431,7 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

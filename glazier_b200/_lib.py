@@ -171,6 +171,18 @@ def _declare_extras(L) -> None:
     L.glz_ens_stream.argtypes = [_P]
     L.glz_ens_destroy.restype = None
     L.glz_ens_destroy.argtypes = [_P]
+    L.glz_adj_create.restype = C.c_int
+    L.glz_adj_create.argtypes = [C.c_int] * 7 + [C.POINTER(_P)]
+    L.glz_adj_set_trajectory.restype = C.c_int
+    L.glz_adj_set_trajectory.argtypes = [_P, _P]
+    L.glz_adj_forward.restype = C.c_int
+    L.glz_adj_forward.argtypes = [_P, _P, _P, _P]
+    L.glz_adj_backward.restype = C.c_int
+    L.glz_adj_backward.argtypes = [_P, _P, _P, _P]
+    L.glz_adj_stream.restype = C.c_void_p
+    L.glz_adj_stream.argtypes = [_P]
+    L.glz_adj_destroy.restype = None
+    L.glz_adj_destroy.argtypes = [_P]
 
 
 def last_error() -> str:

@@ -1,0 +1,607 @@
+// The adjoint of the chemical-field step, conditioned on a recorded lattice
+// trajectory, behind glz_adj_* in include/glazier_gpu.h.
+//
+// Forward, one Monte Carlo step per species s (the engine's field step,
+// field.rs:99-149, in its f32 operation order):
+//   k_s sub-steps   u' = u + d (sum of faces - faces u) - e u,  d = D/k, e = decay/k
+//   exchange        v1 = u + sec[t];  v2 = v1 - upt[t] v1;  v = max(v2, 0)
+// on sites owned by a cell of type t (owner 255 is the medium: no exchange).
+// The discrete Metropolis sweep itself is never differentiated: the owners of
+// every step come from a trajectory the caller recorded.
+//
+// Backward, per step in reverse, per species:
+//   exchange        lambda_v1 = lambda_v [v2 >= 0] (1 - upt);  d/dsec += lambda_v1;
+//                   d/dupt += -lambda_v [v2 >= 0] v1
+//   sub-step        lambda_u = lambda' + d (sum of faces of lambda' - faces lambda') - e lambda'
+//                   (the periodic Laplacian is its own transpose);
+//                   d/dd += lambda' (sum of faces of u - faces u);  d/de += -lambda' u
+// and dD = dd / k, d(decay) = de / k. The forward state is kept at every
+// `checkpoint_every`-th step; the backward recomputes each segment's sub-step
+// inputs from its checkpoint. Adjoint fields are f32; parameter gradients are
+// summed in f64 in an order fixed by the lattice alone.
+//
+// One launch runs one sub-step round of every species that has a sub-step
+// left (the engine's round structure), so with one sub-step per species a
+// step is one launch forward and one backward. The backward of a species'
+// last round applies the exchange adjoint on the fly at the site and its
+// faces (it is pointwise), so it needs no launch of its own.
+//
+// No reference counterpart: glazier has no differentiable field step.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/glazier_gpu.h"
+#include "device.cuh"
+#include "engine.h"
+
+namespace {
+
+int fail(int code, const std::string &msg) {
+    glz::set_last_error(msg);
+    return code;
+}
+
+#define CU(call)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) return fail(GLZ_DRIVER, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kThreads = 256;
+constexpr uint8_t kMedium = 255;
+
+struct Grid {
+    int w, h, d, dim, sites;
+};
+
+__device__ __forceinline__ void faces_of(const Grid &g, size_t i, size_t nb[6]) {
+    const int W = g.w, H = g.h, D = g.d;
+    const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((size_t)W * H));
+    const size_t row = ((size_t)z * H + y) * W;
+    nb[0] = row + (x == 0 ? W - 1 : x - 1);
+    nb[1] = row + (x == W - 1 ? 0 : x + 1);
+    nb[2] = ((size_t)z * H + (y == 0 ? H - 1 : y - 1)) * W + x;
+    nb[3] = ((size_t)z * H + (y == H - 1 ? 0 : y + 1)) * W + x;
+    if (g.dim == 3) {
+        nb[4] = ((size_t)(z == 0 ? D - 1 : z - 1) * H + y) * W + x;
+        nb[5] = ((size_t)(z == D - 1 ? 0 : z + 1) * H + y) * W + x;
+    }
+}
+
+__device__ __forceinline__ float face_sum(const Grid &g, const float *u, const size_t nb[6]) {
+    float sum = u[nb[0]];
+    sum = __fadd_rn(sum, u[nb[1]]);
+    sum = __fadd_rn(sum, u[nb[2]]);
+    sum = __fadd_rn(sum, u[nb[3]]);
+    if (g.dim == 3) {
+        sum = __fadd_rn(sum, u[nb[4]]);
+        sum = __fadd_rn(sum, u[nb[5]]);
+    }
+    return sum;
+}
+
+struct Species {
+    const float *in;    // the sub-step's input
+    float *out;         // its output (after the exchange in the last round); may be null
+    float *keep;        // last round: where to keep the exchange input; may be null
+    float d, e;
+    int active, last;
+};
+
+struct ForwardRound {
+    Grid g;
+    int n_species;
+    const uint8_t *owner;  // this step's owner types
+    const float *sec, *upt;
+    Species sp[glz::kMaxSpecies];
+};
+
+// One sub-step round of the field step; the exchange on a species' last round.
+__global__ void __launch_bounds__(kThreads) forward_round(const __grid_constant__ ForwardRound a) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)a.g.sites) return;
+    size_t nb[6];
+    faces_of(a.g, i, nb);
+    const float faces = a.g.dim == 3 ? 6.0f : 4.0f;
+    int t = -1;
+    for (int s = 0; s < a.n_species; ++s) {
+        const Species &p = a.sp[s];
+        if (!p.active) continue;
+        const float here = p.in[i];
+        const float sum = face_sum(a.g, p.in, nb);
+        float v = __fsub_rn(__fadd_rn(here, __fmul_rn(p.d, __fsub_rn(sum, __fmul_rn(faces, here)))),
+                            __fmul_rn(p.e, here));
+        if (p.last) {
+            if (p.keep) p.keep[i] = v;
+            if (t < 0) t = a.owner[i];
+            if (t != kMedium) {
+                v = __fadd_rn(v, a.sec[t * a.n_species + s]);
+                v = __fsub_rn(v, __fmul_rn(a.upt[t * a.n_species + s], v));
+                v = v < 0.0f ? 0.0f : v;
+            }
+        }
+        if (p.out) p.out[i] = v;
+    }
+}
+
+// Parameter gradients are summed without atomics, in an order fixed by the
+// lattice alone, so a backward is bit-reproducible and independent of the
+// checkpoint interval: the backward kernel runs on a fixed grid of at most
+// `kBlocks` blocks striding over the sites, each block adds its own totals
+// into its own row of `partial` (blocks x n_grads f64; a row is touched by
+// one block only and launches are ordered on one stream), and
+// `reduce_partials` sums the rows in block order at the end.
+constexpr int kBlocks = 148 * 8;
+constexpr int kWarps = kThreads / 32;
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// The block's sum of one f64 per thread, in a fixed order, on thread 0.
+__device__ __forceinline__ double block_sum(double v, double *scratch) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    double total = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kWarps; ++w) total += scratch[w];
+    __syncthreads();
+    return total;
+}
+
+struct Adjoint {
+    const float *u;     // the sub-step's input
+    const float *exch;  // last round: the exchange input
+    const float *lam;   // the adjoint of the round's output (of the step's output in the last round)
+    float *lam_in;      // the adjoint of the sub-step's input
+    float d, e;
+    int active, last;
+};
+
+struct BackwardRound {
+    Grid g;
+    int n_species, n_types, n_grads;
+    const uint8_t *owner;
+    const float *sec, *upt;
+    double *partial;
+    Adjoint sp[glz::kMaxSpecies];
+};
+
+// The exchange adjoint at site j: the adjoint of the exchange input from the
+// adjoint `l` of its output, with v1 and the clamp gate for the gradients.
+__device__ __forceinline__ float exchange_adjoint(const BackwardRound &a, const Adjoint &p, int s, size_t j, float l,
+                                                  float *v1_out, float *lv_out) {
+    const uint8_t t = a.owner[j];
+    if (t == kMedium) return l;
+    const float q = a.upt[t * a.n_species + s];
+    const float v1 = __fadd_rn(p.exch[j], a.sec[t * a.n_species + s]);
+    const float v2 = __fsub_rn(v1, __fmul_rn(q, v1));
+    const float lv = v2 < 0.0f ? 0.0f : l;
+    if (v1_out) {
+        *v1_out = v1;
+        *lv_out = lv;
+    }
+    return __fmul_rn(lv, __fsub_rn(1.0f, q));
+}
+
+// One sub-step round backward, last rounds first: lambda of every active
+// species through its exchange (last round) and sub-step, and the gradients.
+// Each warp reduces the exchange gradients of one owner type at a time (the
+// types present in its 32 sites, in lane order of first appearance); lane 0
+// adds them to the warp's own shared row.
+__global__ void __launch_bounds__(kThreads) backward_round(const __grid_constant__ BackwardRound a) {
+    extern __shared__ double acc[];  // kWarps rows of 2 * n_types: sec then upt
+    __shared__ double scratch[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int T = a.n_types, S = a.n_species;
+    const float faces = a.g.dim == 3 ? 6.0f : 4.0f;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    double *row = a.partial + (size_t)blockIdx.x * a.n_grads;
+    double *mine = acc + (size_t)warp * 2 * T;
+    for (int s = 0; s < S; ++s) {
+        const Adjoint &p = a.sp[s];
+        if (!p.active) continue;
+        if (p.last) {
+            for (int k = threadIdx.x; k < kWarps * 2 * T; k += blockDim.x) acc[k] = 0.0;
+            __syncthreads();
+        }
+        double gd = 0.0, ge = 0.0;
+        // every lane of a warp takes the same number of trips
+        for (size_t base = (size_t)blockIdx.x * blockDim.x; base < (size_t)a.g.sites; base += stride) {
+            const size_t i = base + threadIdx.x;
+            const bool in = i < (size_t)a.g.sites;
+            float l1 = 0.0f, dupt = 0.0f;
+            int t = kMedium;
+            if (in) {
+                size_t nb[6];
+                faces_of(a.g, i, nb);
+                float l = p.lam[i];
+                float ls;
+                if (p.last) {
+                    float v1 = 0.0f, lv = 0.0f;
+                    t = a.owner[i];
+                    l = exchange_adjoint(a, p, s, i, l, &v1, &lv);
+                    if (t != kMedium) {
+                        l1 = l;
+                        dupt = -__fmul_rn(lv, v1);
+                    }
+                    ls = exchange_adjoint(a, p, s, nb[0], p.lam[nb[0]], nullptr, nullptr);
+                    const int nf = a.g.dim == 3 ? 6 : 4;
+                    for (int f = 1; f < nf; ++f)
+                        ls = __fadd_rn(ls, exchange_adjoint(a, p, s, nb[f], p.lam[nb[f]], nullptr, nullptr));
+                } else {
+                    ls = face_sum(a.g, p.lam, nb);
+                }
+                p.lam_in[i] =
+                    __fsub_rn(__fadd_rn(l, __fmul_rn(p.d, __fsub_rn(ls, __fmul_rn(faces, l)))), __fmul_rn(p.e, l));
+                const float here = p.u[i];
+                const float us = face_sum(a.g, p.u, nb);
+                gd += (double)__fmul_rn(l, __fsub_rn(us, __fmul_rn(faces, here)));
+                ge -= (double)__fmul_rn(l, here);
+            }
+            if (p.last) {
+                unsigned todo = __ballot_sync(0xffffffffu, t != kMedium);
+                while (todo) {
+                    const int leader = __ffs(todo) - 1;
+                    const int tt = __shfl_sync(0xffffffffu, t, leader);
+                    const bool same = t == tt;
+                    const double x = warp_sum(same ? (double)l1 : 0.0);
+                    const double y = warp_sum(same ? (double)dupt : 0.0);
+                    if (lane == 0) {
+                        mine[tt] += x;
+                        mine[T + tt] += y;
+                    }
+                    todo &= ~__ballot_sync(0xffffffffu, same);
+                }
+            }
+        }
+        // gradient layout: d, e per species, then sec, upt per (type, species)
+        const double td = block_sum(gd, scratch);
+        const double te = block_sum(ge, scratch);
+        if (threadIdx.x == 0) {
+            row[s] += td;
+            row[S + s] += te;
+        }
+        if (p.last) {
+            __syncthreads();
+            for (int k = threadIdx.x; k < 2 * T; k += blockDim.x) {
+                double v = 0.0;
+                for (int w = 0; w < kWarps; ++w) v += acc[(size_t)w * 2 * T + k];
+                const int tt = k % T;
+                row[(k < T ? 2 * S : 2 * S + T * S) + tt * S + s] += v;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// grads[k] = the sum over blocks of partial[b][k], in block order.
+__global__ void reduce_partials(const double *__restrict__ partial, int blocks, int n_grads,
+                                double *__restrict__ grads) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_grads) return;
+    double v = 0.0;
+    for (int b = 0; b < blocks; ++b) v += partial[(size_t)b * n_grads + k];
+    grads[k] = v;
+}
+
+// field.rs:155-160
+int substeps(double diffusion, int dimensions) {
+    if (diffusion <= 0.0) return 1;
+    double k = std::ceil(diffusion / (1.0 / (2.0 * (double)dimensions)));
+    return k < 1.0 ? 1 : (int)k;
+}
+
+}  // namespace
+
+struct glz_adj {
+    Grid g{};
+    int n_species = 0, n_types = 0, steps = 0, every = 1;
+    cudaStream_t stream = nullptr;
+    uint8_t *owner = nullptr;  // steps * sites
+    bool have_trajectory = false;
+    float *ckpt = nullptr;     // ceil(steps / every) checkpoints of n_species * sites
+    float *seg = nullptr;      // a segment's sub-step states: every * (kmax + 1) * n_species * sites
+    float *tmp[2] = {};        // n_species * sites each: sub-step outputs inside a step
+    float *work[2] = {};       // step outputs between checkpoints
+    float *lam[2] = {};        // the adjoint fields
+    float *d_sec = nullptr, *d_upt = nullptr;
+    double *partial = nullptr;  // kBlocks rows of n_grads
+    double *d_grads = nullptr;  // n_grads: d, e per species, then sec, upt per (type, species)
+    std::vector<double> params;
+    std::vector<int> k;
+    int kmax = 0;
+    int seg_kmax = -1;          // the kmax `seg` was sized for
+    bool forward_done = false;
+};
+
+namespace {
+
+size_t field_floats(const glz_adj *h) { return (size_t)h->n_species * h->g.sites; }
+int n_grads(const glz_adj *h) { return 2 * h->n_species + 2 * h->n_types * h->n_species; }
+int blocks_for(const glz_adj *h) { return (int)((h->g.sites + kThreads - 1) / kThreads); }
+
+// The sub-step state j of species s at step `local` of the segment starting
+// at checkpoint `sg`: j < k[s] the input of sub-step j, j = k[s] the exchange
+// input. State 0 of the segment's first step is the checkpoint itself.
+float *seg_state(glz_adj *h, int sg, int local, int j, int s) {
+    if (local == 0 && j == 0) return h->ckpt + ((size_t)sg * h->n_species + s) * (size_t)h->g.sites;
+    return h->seg + (((size_t)local * (h->kmax + 1) + j) * h->n_species + s) * (size_t)h->g.sites;
+}
+
+int set_params(glz_adj *h, const double *params) {
+    const int S = h->n_species, T = h->n_types;
+    for (int s = 0; s < S; ++s)
+        if (!(params[s] >= 0.0) || !(params[S + s] >= 0.0) || !std::isfinite(params[s]) ||
+            !std::isfinite(params[S + s]))
+            return fail(GLZ_INVALID, "diffusion and decay must be finite and >= 0");
+    h->params.assign(params, params + n_grads(h));
+    h->k.resize(S);
+    h->kmax = 0;
+    for (int s = 0; s < S; ++s) {
+        h->k[s] = substeps(params[s], h->g.dim);
+        h->kmax = h->k[s] > h->kmax ? h->k[s] : h->kmax;
+    }
+    std::vector<float> sec(T * S), upt(T * S);
+    for (int i = 0; i < T * S; ++i) {
+        sec[i] = (float)params[2 * S + i];
+        upt[i] = (float)params[2 * S + T * S + i];
+    }
+    CU(cudaMemcpyAsync(h->d_sec, sec.data(), sec.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->d_upt, upt.data(), upt.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    // the host vectors must outlive the copies
+    CU(cudaStreamSynchronize(h->stream));
+    if (h->seg_kmax != h->kmax) {
+        cudaFree(h->seg);
+        h->seg = nullptr;
+        h->seg_kmax = -1;
+        CU(cudaMalloc(&h->seg, (size_t)h->every * (h->kmax + 1) * field_floats(h) * sizeof(float)));
+        h->seg_kmax = h->kmax;
+    }
+    return GLZ_OK;
+}
+
+float d_of(const glz_adj *h, int s) { return (float)(h->params[s] / (double)h->k[s]); }
+float e_of(const glz_adj *h, int s) { return (float)(h->params[h->n_species + s] / (double)h->k[s]); }
+
+// One step forward of every species, owners of step t, from `in` to `out`
+// (n_species * sites each, distinct buffers).
+int step_forward(glz_adj *h, int t, const float *in, float *out) {
+    const size_t n = h->g.sites;
+    ForwardRound a{};
+    a.g = h->g;
+    a.n_species = h->n_species;
+    a.owner = h->owner + (size_t)t * n;
+    a.sec = h->d_sec;
+    a.upt = h->d_upt;
+    const float *cur[glz::kMaxSpecies];
+    for (int s = 0; s < h->n_species; ++s) cur[s] = in + (size_t)s * n;
+    for (int r = 0; r < h->kmax; ++r) {
+        for (int s = 0; s < h->n_species; ++s) {
+            Species &p = a.sp[s];
+            p.active = r < h->k[s];
+            p.last = r == h->k[s] - 1;
+            p.d = d_of(h, s);
+            p.e = e_of(h, s);
+            p.in = cur[s];
+            p.keep = nullptr;
+            p.out = p.last ? out + (size_t)s * n : h->tmp[r & 1] + (size_t)s * n;
+            if (p.active) cur[s] = p.out;
+        }
+        forward_round<<<blocks_for(h), kThreads, 0, h->stream>>>(a);
+    }
+    CU(cudaGetLastError());
+    return GLZ_OK;
+}
+
+// Recompute segment `sg`, keeping every sub-step state; its last step's
+// output is not needed.
+int recompute(glz_adj *h, int sg, int len) {
+    ForwardRound a{};
+    a.g = h->g;
+    a.n_species = h->n_species;
+    a.sec = h->d_sec;
+    a.upt = h->d_upt;
+    for (int local = 0; local < len; ++local) {
+        a.owner = h->owner + (size_t)(sg * h->every + local) * h->g.sites;
+        for (int r = 0; r < h->kmax; ++r) {
+            for (int s = 0; s < h->n_species; ++s) {
+                Species &p = a.sp[s];
+                p.active = r < h->k[s];
+                p.last = r == h->k[s] - 1;
+                p.d = d_of(h, s);
+                p.e = e_of(h, s);
+                if (!p.active) continue;
+                p.in = seg_state(h, sg, local, r, s);
+                if (p.last) {
+                    p.keep = seg_state(h, sg, local, h->k[s], s);
+                    p.out = local + 1 < len ? seg_state(h, sg, local + 1, 0, s) : nullptr;
+                } else {
+                    p.keep = nullptr;
+                    p.out = seg_state(h, sg, local, r + 1, s);
+                }
+            }
+            forward_round<<<blocks_for(h), kThreads, 0, h->stream>>>(a);
+        }
+    }
+    CU(cudaGetLastError());
+    return GLZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int glz_adj_create(int width, int height, int depth, int n_species, int n_types, int steps, int checkpoint_every,
+                   glz_adj **out) {
+    if (!out) return fail(GLZ_INVALID, "null output handle");
+    *out = nullptr;
+    if (width <= 0 || height <= 0 || depth <= 0) return fail(GLZ_INVALID, "the lattice has a zero dimension");
+    if (n_species < 1 || n_species > glz::kMaxSpecies || n_types < 1 || n_types > 254 || steps < 1 ||
+        checkpoint_every < 1)
+        return fail(GLZ_INVALID, "species 1..8, types 1..254, steps and checkpoint interval >= 1");
+    const long long sites = (long long)width * height * depth;
+    if (sites >= (1LL << 31)) return fail(GLZ_INVALID, "the lattice has 2^31 sites or more");
+    glz_adj *h = new glz_adj();
+    h->g = Grid{width, height, depth, depth > 1 ? 3 : 2, (int)sites};
+    h->n_species = n_species;
+    h->n_types = n_types;
+    h->steps = steps;
+    h->every = checkpoint_every < steps ? checkpoint_every : steps;
+    const size_t n = field_floats(h);
+    const int nckpt = (steps + h->every - 1) / h->every;
+    auto bail = [&](int rc) {
+        glz_adj_destroy(h);
+        return rc;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&h->owner, (size_t)steps * sites) != cudaSuccess ||
+        cudaMalloc(&h->ckpt, (size_t)nckpt * n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->tmp[0], n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->tmp[1], n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->work[0], n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->work[1], n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->lam[0], n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->lam[1], n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->d_sec, (size_t)n_types * n_species * 4) != cudaSuccess ||
+        cudaMalloc(&h->d_upt, (size_t)n_types * n_species * 4) != cudaSuccess ||
+        cudaMalloc(&h->partial, (size_t)kBlocks * n_grads(h) * 8) != cudaSuccess ||
+        cudaMalloc(&h->d_grads, (size_t)n_grads(h) * 8) != cudaSuccess)
+        return bail(fail(GLZ_DRIVER, "adjoint allocation failed"));
+    *out = h;
+    return GLZ_OK;
+}
+
+int glz_adj_set_trajectory(glz_adj *h, const uint8_t *owner_types) {
+    if (!h || !owner_types) return fail(GLZ_INVALID, "null handle or trajectory");
+    const size_t bytes = (size_t)h->steps * h->g.sites;
+    for (size_t i = 0; i < bytes; ++i)
+        if (owner_types[i] != kMedium && owner_types[i] >= h->n_types)
+            return fail(GLZ_INVALID, "an owner type past the type count (255 is the medium)");
+    CU(cudaMemcpyAsync(h->owner, owner_types, bytes, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    h->have_trajectory = true;
+    h->forward_done = false;
+    return GLZ_OK;
+}
+
+int glz_adj_forward(glz_adj *h, const double *params, const float *fields0, float *fields_final) {
+    if (!h || !params || !fields0 || !fields_final) return fail(GLZ_INVALID, "null argument");
+    if (!h->have_trajectory) return fail(GLZ_INVALID, "no trajectory set");
+    if (fields0 == fields_final) return fail(GLZ_INVALID, "the initial and final fields share a buffer");
+    h->forward_done = false;
+    if (int rc = set_params(h, params)) return rc;
+    const size_t n = field_floats(h);
+    // checkpoint 0 is the start; a step's output goes to the next checkpoint,
+    // to the work buffer the step did not read, or (the last) to the caller
+    CU(cudaMemcpyAsync(h->ckpt, fields0, n * 4, cudaMemcpyDeviceToDevice, h->stream));
+    const float *cur = h->ckpt;
+    for (int t = 0; t < h->steps; ++t) {
+        float *dst;
+        if (t == h->steps - 1)
+            dst = fields_final;
+        else if ((t + 1) % h->every == 0)
+            dst = h->ckpt + (size_t)((t + 1) / h->every) * n;
+        else
+            dst = cur == h->work[0] ? h->work[1] : h->work[0];
+        if (int rc = step_forward(h, t, cur, dst)) return rc;
+        cur = dst;
+    }
+    CU(cudaStreamSynchronize(h->stream));
+    h->forward_done = true;
+    return GLZ_OK;
+}
+
+int glz_adj_backward(glz_adj *h, const float *grad_final, double *grad_params, float *grad_fields0) {
+    if (!h || !grad_final || !grad_params) return fail(GLZ_INVALID, "null argument");
+    if (!h->forward_done) return fail(GLZ_INVALID, "backward before forward");
+    const int S = h->n_species, T = h->n_types, G = n_grads(h);
+    const size_t n = field_floats(h), sites = h->g.sites;
+    const int grid = blocks_for(h) < kBlocks ? blocks_for(h) : kBlocks;
+    CU(cudaMemsetAsync(h->partial, 0, (size_t)grid * G * 8, h->stream));
+    CU(cudaMemcpyAsync(h->lam[0], grad_final, n * 4, cudaMemcpyDeviceToDevice, h->stream));
+    int cur[glz::kMaxSpecies] = {};  // which lam buffer holds each species' adjoint
+    BackwardRound a{};
+    a.g = h->g;
+    a.n_species = S;
+    a.n_types = T;
+    a.n_grads = G;
+    a.sec = h->d_sec;
+    a.upt = h->d_upt;
+    a.partial = h->partial;
+    const size_t smem = (size_t)kWarps * 2 * T * sizeof(double);
+    const int nseg = (h->steps + h->every - 1) / h->every;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int t0 = sg * h->every, len = (t0 + h->every < h->steps ? t0 + h->every : h->steps) - t0;
+        if (int rc = recompute(h, sg, len)) return rc;
+        for (int local = len - 1; local >= 0; --local) {
+            a.owner = h->owner + (size_t)(t0 + local) * sites;
+            for (int r = h->kmax - 1; r >= 0; --r) {
+                for (int s = 0; s < S; ++s) {
+                    Adjoint &p = a.sp[s];
+                    p.active = r < h->k[s];
+                    p.last = r == h->k[s] - 1;
+                    p.d = d_of(h, s);
+                    p.e = e_of(h, s);
+                    if (!p.active) continue;
+                    p.u = seg_state(h, sg, local, r, s);
+                    p.exch = seg_state(h, sg, local, h->k[s], s);
+                    p.lam = h->lam[cur[s]] + (size_t)s * sites;
+                    p.lam_in = h->lam[1 - cur[s]] + (size_t)s * sites;
+                    cur[s] = 1 - cur[s];
+                }
+                backward_round<<<grid, kThreads, smem, h->stream>>>(a);
+            }
+        }
+        CU(cudaGetLastError());
+    }
+    reduce_partials<<<(G + 127) / 128, 128, 0, h->stream>>>(h->partial, grid, G, h->d_grads);
+    CU(cudaGetLastError());
+    if (grad_fields0)
+        for (int s = 0; s < S; ++s)
+            CU(cudaMemcpyAsync(grad_fields0 + (size_t)s * sites, h->lam[cur[s]] + (size_t)s * sites, sites * 4,
+                               cudaMemcpyDeviceToDevice, h->stream));
+    std::vector<double> g(G);
+    CU(cudaMemcpyAsync(g.data(), h->d_grads, (size_t)G * 8, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    // d = D / k and e = decay / k, so the D and decay gradients are the
+    // per-sub-step ones over k
+    for (int s = 0; s < S; ++s) {
+        grad_params[s] = g[s] / h->k[s];
+        grad_params[S + s] = g[S + s] / h->k[s];
+    }
+    for (int i = 2 * S; i < G; ++i) grad_params[i] = g[i];
+    return GLZ_OK;
+}
+
+void *glz_adj_stream(glz_adj *h) { return h ? (void *)h->stream : nullptr; }
+
+void glz_adj_destroy(glz_adj *h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->owner);
+    cudaFree(h->ckpt);
+    cudaFree(h->seg);
+    cudaFree(h->tmp[0]);
+    cudaFree(h->tmp[1]);
+    cudaFree(h->work[0]);
+    cudaFree(h->work[1]);
+    cudaFree(h->lam[0]);
+    cudaFree(h->lam[1]);
+    cudaFree(h->d_sec);
+    cudaFree(h->d_upt);
+    cudaFree(h->partial);
+    cudaFree(h->d_grads);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // extern "C"

@@ -13,7 +13,7 @@ import math
 
 import numpy as np
 
-from .blueprint import CellType, Model, Start
+from .blueprint import CellType, Model, Species, Start
 
 _M64 = (1 << 64) - 1
 
@@ -90,3 +90,43 @@ def ensemble_starts(count: int = 64, seed: int = 1, side: int = 8, low: int = 12
         starts.append(monolayer(size, contact=contact, lambda_volume=lambda_volume, temperature=temperature,
                                 seed=(seed * 1_000_003 + i) & _M64, side=side))
     return starts
+
+
+def adjoint_start(seed: int = 1, size: int = 512, side: int = 8) -> Start:
+    """The field-adjoint workload: a periodic `size` lattice tiled by cells of
+    `side` (512^2: 4096 cells), types medium, healthy, infected and immune,
+    with the infection model's two fields: virus (D 0.05, decay 0.01) and
+    interferon (D 0.1, decay 0.005). Infected cells secrete virus at 1.0 and
+    interferon at 0.5 per site per MCS, healthy cells take up virus at 0.02;
+    immune cells climb interferon (chemotaxis 50) under a length term
+    (lambda_L 2, L_target 12). One cell in 16 is infected and 32 are immune,
+    picked by the hash of (seed, cell). J is 10 between cells, 16 against the
+    medium; lambda_V 1 at the tile volume; T 10."""
+    vt = float(side * side)
+    cell = dict(target_volume=vt, lambda_volume=1.0)
+    n = 4
+    contact = [0.0 if (a == 0 and b == 0) else (16.0 if (a == 0 or b == 0) else 10.0)
+               for a in range(n) for b in range(n)]
+    model = Model(
+        width=size,
+        height=size,
+        contact=contact,
+        types=[CellType(), CellType(**cell), CellType(**cell),
+               CellType(target_length=12.0, lambda_length=2.0, **cell)],
+        temperature=10.0,
+        neighbour_order=2,
+        seed=seed,
+        species=[Species("virus", 0.05, 0.01, 0.0), Species("interferon", 0.1, 0.005, 0.0)],
+        secretion=[[0.0, 0.0], [0.0, 0.0], [1.0, 0.5], [0.0, 0.0]],
+        uptake=[[0.0, 0.0], [0.02, 0.0], [0.0, 0.0], [0.0, 0.0]],
+        chemotaxis=[[0.0, 0.0], [0.0, 0.0], [0.0, 0.0], [0.0, 50.0]],
+    )
+    start = Start.tiled(model, side)
+    cells = start.n_cells
+    order = sorted(range(1, cells + 1), key=lambda c: uniform01(seed, c, 7))
+    start.cell_type[1:] = 1
+    for c in order[: cells // 16]:
+        start.cell_type[c] = 2
+    for c in order[cells // 16: cells // 16 + 32]:
+        start.cell_type[c] = 3
+    return start

@@ -182,6 +182,38 @@ uint64_t glz_ens_mcs(const glz_ens *h);
 void *glz_ens_stream(glz_ens *h);
 void glz_ens_destroy(glz_ens *h);
 
+/* ---------------------------------------------------------------- field adjoint
+ *
+ * The chemical-field step differentiated with respect to its parameters,
+ * conditioned on a recorded lattice trajectory (the Metropolis sweep itself is
+ * never differentiated). No reference counterpart. The forward is the
+ * engine's own field step in f32 (one MCS per trajectory step); the backward
+ * is its hand-written adjoint, recomputing each segment of `checkpoint_every`
+ * steps from a saved state.
+ *
+ * Parameters, f64, 2 S + 2 T S values: D[S], decay[S], secretion[T][S],
+ * uptake[T][S] (S species, T types, row-major). A trajectory is steps * sites
+ * owner types, 255 for the medium.
+ */
+typedef struct glz_adj glz_adj;
+
+int glz_adj_create(int width, int height, int depth, int n_species, int n_types, int steps, int checkpoint_every,
+                   glz_adj **out);
+/* owner_types: host, steps * sites. */
+int glz_adj_set_trajectory(glz_adj *h, const uint8_t *owner_types);
+/* fields0, fields_final: device, n_species * sites f32, species-major,
+ * distinct buffers. Returns once the fields are written. */
+int glz_adj_forward(glz_adj *h, const double *params, const float *fields0, float *fields_final);
+/* grad_final: device, the loss gradient at the final fields; grad_params:
+ * host, 2 S + 2 T S values; grad_fields0: device or NULL. Uses the
+ * parameters of the last forward. Gradients are summed in an order fixed by
+ * the lattice, so they are the same bits for every checkpoint interval and
+ * every run. */
+int glz_adj_backward(glz_adj *h, const float *grad_final, double *grad_params, float *grad_fields0);
+/* The CUDA stream (a cudaStream_t) all of the handle's work runs on. */
+void *glz_adj_stream(glz_adj *h);
+void glz_adj_destroy(glz_adj *h);
+
 /* The most f32 values of intermediate fields glz_field_step_noalloc holds:
  * 4,194,304 (16 MiB), beside a table area of 1,024 values. */
 #define GLZ_NOALLOC_FIELD_SCRATCH (1u << 22)

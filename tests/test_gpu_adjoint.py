@@ -1,0 +1,251 @@
+"""The field adjoint: its forward against the engine, its gradient against f64.
+
+The forward, driven by the owner trajectory an engine run records, must land
+on the engine's own f32 fields bit for bit. The f32 adjoint gradient of an
+MSE loss against the f64 forward at parameters perturbed by 10% must match
+PyTorch f64 autograd of a plain stencil and FP64 central finite differences
+(h = 1e-6) to 1e-4 relative in the infinity norm over the parameters (and
+each component to 1e-3 of itself plus 1e-5 of the largest), and must be bit-identical for every checkpoint
+interval, since its sums run in a fixed order.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from glazier_b200.blueprint import CellType, Model, Species, Start
+
+pytestmark = pytest.mark.gpu
+
+# (width, height, depth, cell side, cells per axis, steps, diffusion per species)
+CASES = {
+    # D 0.3 takes two sub-steps in a plane, 0.1 one; medium along two edges
+    "plane": (64, 48, 1, 8, (7, 5, 1), 12, (0.3, 0.1)),
+    # D 0.2 takes two sub-steps in 3D (limit 1/6), 0.05 one
+    "cube": (16, 16, 12, 4, (4, 4, 2), 7, (0.2, 0.05)),
+}
+
+
+def _model(case) -> Model:
+    w, h, d, side, _, _, diff = CASES[case]
+    vt = float(side ** (3 if d > 1 else 2))
+    return Model(
+        width=w,
+        height=h,
+        depth=d,
+        contact=[0.0, 16.0, 16.0, 16.0, 8.0, 10.0, 16.0, 10.0, 8.0],
+        types=[CellType(), CellType(target_volume=vt, lambda_volume=2.0),
+               CellType(target_volume=0.75 * vt, lambda_volume=2.0)],
+        temperature=10.0,
+        neighbour_order=2,
+        seed=17,
+        species=[Species("virus", diff[0], 0.01, 0.0), Species("interferon", diff[1], 0.02, 0.0)],
+        secretion=[[0.0, 0.0], [0.05, 0.0], [0.3, 0.2]],
+        uptake=[[0.0, 0.0], [0.02, 0.01], [0.0, 0.03]],
+        chemotaxis=[[0.0, 0.0], [0.0, 0.0], [0.0, 0.0]],
+    )
+
+
+def _params(m: Model) -> np.ndarray:
+    """D and decay per species, then secretion and uptake per type and species."""
+    return np.concatenate([[s.diffusion for s in m.species], [s.decay for s in m.species],
+                           np.asarray(m.secretion, dtype=np.float64).reshape(-1),
+                           np.asarray(m.uptake, dtype=np.float64).reshape(-1)])
+
+
+def _torch_forward(params, f0, traj, n_types, shape):
+    """The field step in plain f64 PyTorch: rolls for the Laplacian, masks for
+    the exchange. `shape` is (depth, height, width)."""
+    import torch
+
+    S = f0.shape[0]
+    dim = 3 if shape[0] > 1 else 2
+    axes = (0, 1, 2) if dim == 3 else (1, 2)
+    D, dec = params[:S], params[S:2 * S]
+    sec = params[2 * S:2 * S + n_types * S].reshape(n_types, S)
+    upt = params[2 * S + n_types * S:].reshape(n_types, S)
+    f = [f0[s].reshape(shape) for s in range(S)]
+    for t in range(traj.shape[0]):
+        own = torch.from_numpy(traj[t].astype(np.int64)).reshape(shape)
+        owned = own != 255
+        idx = torch.where(owned, own, torch.zeros_like(own))
+        nxt = []
+        for s in range(S):
+            dv = float(D[s].detach())
+            k = max(1, math.ceil(dv / (1.0 / (2 * dim)))) if dv > 0 else 1
+            d, e = D[s] / k, dec[s] / k
+            u = f[s]
+            for _ in range(k):
+                lap = -2.0 * dim * u
+                for ax in axes:
+                    lap = lap + torch.roll(u, 1, ax) + torch.roll(u, -1, ax)
+                u = u + d * lap - e * u
+            v1 = u + sec[idx, s]
+            v2 = v1 - upt[idx, s] * v1
+            nxt.append(torch.where(owned, torch.clamp(v2, min=0.0), u))
+        f = nxt
+    return torch.stack([x.reshape(-1) for x in f])
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def recorded(request, device):
+    """An engine run of the case's steps with two species: its start, initial
+    fields, owner trajectory and final f32 fields."""
+    from glazier_b200.adjoint import record_trajectory
+
+    case = request.param
+    _, _, _, side, (nx, ny, nz), steps, _ = CASES[case]
+    m = _model(case)
+    st = Start.tiled_grid(m, side, nx, ny, nz)
+    st.cell_type[1::3] = 2
+    f0 = np.random.default_rng(3).uniform(0.5, 2.0, size=(2, m.sites))
+    sim = device.GpuSimulation.from_start(st, f0)
+    traj = record_trajectory(sim, steps)
+    final = np.stack([sim.field(k) for k in range(2)]).astype(np.float32)
+    sim.close()
+    assert (traj == 255).any() and (traj == 1).any() and (traj == 2).any()
+    return st, f0, traj, final
+
+
+def _adjoint(st, traj, every):
+    from glazier_b200.adjoint import FieldAdjoint
+
+    m = st.model
+    return FieldAdjoint(m.width, m.height, m.depth, 2, m.n_types, traj, checkpoint_every=every)
+
+
+def _shape(st):
+    return (st.model.depth, st.model.height, st.model.width)
+
+
+def test_the_forward_is_the_engines_field_step(recorded):
+    import torch
+
+    st, f0, traj, final = recorded
+    adj = _adjoint(st, traj, 5)
+    out = adj.forward(_params(st.model), torch.from_numpy(f0.astype(np.float32)).cuda())
+    assert np.array_equal(out.cpu().numpy(), final)
+    adj.close()
+
+
+def _target(st, traj, f0):
+    """The MSE target: the f64 forward at parameters perturbed by 10%
+    uniform noise."""
+    import torch
+
+    p = _params(st.model)
+    perturbed = p * (1.0 + 0.1 * np.random.default_rng(11).uniform(-1.0, 1.0, size=p.size))
+    return _torch_forward(torch.from_numpy(perturbed), torch.from_numpy(f0), traj, st.model.n_types, _shape(st))
+
+
+def _device_gradient(st, traj, f0, target, every):
+    import torch
+
+    adj = _adjoint(st, traj, every)
+    out = adj.forward(_params(st.model), torch.from_numpy(f0.astype(np.float32)).cuda())
+    grad_final = 2.0 * (out - target.to(torch.float32).cuda()) / out.numel()
+    gp, gf = adj.backward(grad_final)
+    adj.close()
+    return gp, gf
+
+
+def test_the_adjoint_matches_f64_autograd_and_finite_differences(recorded):
+    import torch
+
+    st, f0, traj, _ = recorded
+    target = _target(st, traj, f0)
+    p = _params(st.model)
+    gp, _ = _device_gradient(st, traj, f0, target, every=5)
+    f0_64 = torch.from_numpy(f0)
+
+    def loss(params):
+        out = _torch_forward(params, f0_64, traj, st.model.n_types, _shape(st))
+        return ((out - target) ** 2).mean()
+
+    pt = torch.from_numpy(p.copy()).requires_grad_(True)
+    loss(pt).backward()
+    auto = pt.grad.numpy()
+    scale = np.abs(auto).max()
+    assert scale > 0
+    assert np.abs(gp - auto).max() / scale < 1e-4, (gp, auto)
+    live = np.abs(auto) > 0
+    assert np.all(gp[~live] == 0.0)
+    # component by component, with a floor for sums that nearly cancel
+    assert np.all(np.abs(gp - auto) <= 1e-3 * np.abs(auto) + 1e-5 * scale), (gp, auto)
+
+    h = 1e-6
+    fd = np.zeros_like(p)
+    with torch.no_grad():
+        for i in range(p.size):
+            up, dn = p.copy(), p.copy()
+            up[i] += h
+            dn[i] -= h
+            fd[i] = (loss(torch.from_numpy(up)).item() - loss(torch.from_numpy(dn)).item()) / (2 * h)
+    assert np.abs(gp - fd).max() / np.abs(fd).max() < 1e-4, (gp, fd)
+
+
+def test_the_gradient_does_not_depend_on_the_checkpoint_interval(recorded):
+    st, f0, traj, _ = recorded
+    target = _target(st, traj, f0)
+    base, gf_base = _device_gradient(st, traj, f0, target, every=traj.shape[0])
+    for every in (1, 3, 5):
+        gp, gf = _device_gradient(st, traj, f0, target, every=every)
+        assert np.array_equal(gp, base)
+        assert np.array_equal(gf.cpu().numpy(), gf_base.cpu().numpy())
+
+
+def test_the_initial_field_gradient_matches_autograd(recorded):
+    import torch
+
+    st, f0, traj, _ = recorded
+    target = _target(st, traj, f0)
+    _, gf = _device_gradient(st, traj, f0, target, every=3)
+    f0_64 = torch.from_numpy(f0.copy()).requires_grad_(True)
+    out = _torch_forward(torch.from_numpy(_params(st.model)), f0_64, traj, st.model.n_types, _shape(st))
+    ((out - target) ** 2).mean().backward()
+    auto = f0_64.grad.numpy()
+    assert np.abs(gf.cpu().numpy() - auto).max() / np.abs(auto).max() < 1e-4
+
+
+def test_the_autograd_function_carries_the_gradient(recorded):
+    import torch
+
+    from glazier_b200.adjoint import field_trajectory
+
+    st, f0, traj, _ = recorded
+    target = _target(st, traj, f0)
+    adj = _adjoint(st, traj, 4)
+    params = torch.from_numpy(_params(st.model)).requires_grad_(True)
+    fields0 = torch.from_numpy(f0.astype(np.float32)).cuda().requires_grad_(True)
+    out = field_trajectory(params, fields0, adj)
+    loss = ((out - target.to(torch.float32).cuda()) ** 2).mean()
+    loss.backward()
+    gp, gf = _device_gradient(st, traj, f0, target, every=4)
+    assert np.array_equal(params.grad.numpy(), gp)
+    assert torch.equal(fields0.grad, gf)
+    adj.close()
+
+
+def test_bad_arguments_are_refused(recorded):
+    import torch
+
+    from glazier_b200.adjoint import FieldAdjoint
+    from glazier_b200.engine import GpuError
+
+    st, f0, traj, _ = recorded
+    m = st.model
+    bad = traj.copy()
+    bad[0, 0] = 7  # a type past the three the model has
+    with pytest.raises(GpuError, match="owner type"):
+        FieldAdjoint(m.width, m.height, m.depth, 2, m.n_types, bad)
+    adj = _adjoint(st, traj, 4)
+    with pytest.raises(GpuError, match="backward before forward"):
+        adj.backward(torch.zeros(adj.shape, device="cuda"))
+    p = _params(m)
+    p[0] = -0.1
+    with pytest.raises(GpuError, match="diffusion and decay"):
+        adj.forward(p, torch.from_numpy(f0.astype(np.float32)).cuda())
+    adj.close()
