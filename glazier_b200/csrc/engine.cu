@@ -129,6 +129,7 @@ struct glz_gpu {
     int field_cur[glz::kMaxSpecies] = {};
     uint64_t pass_no = 0, mcs = 0;
     bool use_tma = false;
+    bool lean = false;  // the sweep prices contact, volume and surface only
     int max_ctas = 0;
     int uniform = -1;
     bool uniform_exact = false;
@@ -347,6 +348,7 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.has_chemotaxis = h->has_chemotaxis;
     for (int s = 0; s < h->n_species; ++s) a.fields[s] = h->field_ptr(s, h->field_cur[s]);
     a.use_tma = h->use_tma;
+    a.lean = h->lean;
     a.max_ctas = h->max_ctas;
     a.tensor_map = h->use_tma ? &h->tmap : nullptr;
     a.error_flag = h->error_flag;
@@ -590,6 +592,9 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         }
     }
 
+    // GLAZIER_SWEEP_LEAN=0 keeps every model on the general sweep kernel.
+    const char *lean_env = std::getenv("GLAZIER_SWEEP_LEAN");
+    h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !has_conn && !(lean_env && lean_env[0] == '0');
     h->host_tv = tv;
     h->host_lv = lv;
     h->host_ts = ts;

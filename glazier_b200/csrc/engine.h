@@ -80,6 +80,7 @@ struct SweepLaunch {
     int has_length, tracks, has_chemotaxis;
     const float *fields[kMaxSpecies];
     int use_tma;
+    int lean;                // take the lean kernel: no length, chemotaxis, connectivity or moment tracking
     int max_ctas;            // > 0 caps the persistent grid (each CTA then walks more tiles)
     const void *tensor_map;  // CUtensorMap in device-visible memory, or null
     int *error_flag;

@@ -308,9 +308,15 @@ __device__ __noinline__ void commit_moments(const SweepLaunch &a, uint32_t old, 
 // counts (the host has checked that J m is exact in f32 for every count m,
 // which makes it the same number the neighbour-by-neighbour sum rounds to)
 // and the per-type constants come from the launch parameters.
-template <int DIM, int NOFF, bool UNIFORM>
-__device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const SweepSmem<DIM> &S, const uint32_t *win,
-                                                 uint32_t entry, int x0, int y0, int z0, bool small_types) {
+//
+// EXTRAS false compiles out the length, chemotaxis, connectivity and moment
+// parts, for launches whose model has none of them. `woff`, `contact` and
+// `wring` are the shared-memory tables: window offset of each pick, the
+// contact matrix when `small_types`, the connectivity ring.
+template <int DIM, int NOFF, bool UNIFORM, bool EXTRAS>
+__device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const int *woff, const float *contact,
+                                                 const int *wring, const uint32_t *win, uint32_t entry, int x0,
+                                                 int y0, int z0, bool small_types) {
     using T = Tile<DIM>;
     const int W = a.g.w, H = a.g.h;
     const int j = (int)(entry & 0xffffu);
@@ -321,7 +327,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
     const uint32_t target = (uint32_t)((z * H + y) * W + x);
     const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
     const uint32_t old = win[wc];
-    const uint32_t nw = win[wc + S.woff[pick]];
+    const uint32_t nw = win[wc + woff[pick]];
 
     // The snapshot tallies of both cells, requested before the neighbour loop
     // so their latency hides behind it.
@@ -355,14 +361,14 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
             const int tn = ln == old ? t_old : (ln == nw ? t_new : (int)a.cell_type[ln]);
             if (ln != old) {
                 const float j_old =
-                    small_types ? S.contact[t_old * a.n_types + tn] : a.t.contact[t_old * a.n_types + tn];
+                    small_types ? contact[t_old * a.n_types + tn] : a.t.contact[t_old * a.n_types + tn];
                 delta = __fsub_rn(delta, j_old);
             } else {
                 ++like_old;
             }
             if (ln != nw) {
                 const float j_new =
-                    small_types ? S.contact[t_new * a.n_types + tn] : a.t.contact[t_new * a.n_types + tn];
+                    small_types ? contact[t_new * a.n_types + tn] : a.t.contact[t_new * a.n_types + tn];
                 delta = __fadd_rn(delta, j_new);
             } else {
                 ++like_new;
@@ -374,7 +380,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
         // A like neighbour is a site of another colour, since every neighbour
         // of a target is; only a target with none needs the per-colour count.
         if (like_old == 0 && !keeps_other_colour(a, old)) return;
-        if (a.g.ring_n > 0 && a.t.connected[t_old] && !ring_one_piece(a, S.wring, win, wc, old)) return;
+        if (EXTRAS && a.g.ring_n > 0 && a.t.connected[t_old] && !ring_one_piece(a, wring, win, wc, old)) return;
     }
     const int ds_old = 2 * like_old - NOFF;
     const int ds_new = NOFF - 2 * like_new;
@@ -421,7 +427,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
         }
     }
-    if (a.has_length || a.has_chemotaxis)
+    if (EXTRAS && (a.has_length || a.has_chemotaxis))
         delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
 
     if (delta > 0.0f) {
@@ -438,7 +444,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const Swe
         atomicAdd(&a.vs_cur[nw], pack_delta(1, ds_new));
         atomicAdd(&a.vol_by_colour[(size_t)nw * a.g.ncol + a.colour], 1);
     }
-    if (a.tracks) commit_moments<DIM>(a, old, nw, x, y, z);
+    if (EXTRAS && a.tracks) commit_moments<DIM>(a, old, nw, x, y, z);
 }
 
 template <int DIM>
@@ -570,7 +576,8 @@ __device__ __forceinline__ void price_tile(const SweepLaunch &a, SweepSmem<DIM> 
         first = __shfl_sync(0xffffffffu, first, 0);
         if (first >= queued) break;
         if (first + lane < queued)
-            price_and_commit<DIM, NOFF, UNIFORM>(a, S, win, S.queue[first + lane], x0, y0, z0, small_types);
+            price_and_commit<DIM, NOFF, UNIFORM, true>(a, S.woff, S.contact, S.wring, win, S.queue[first + lane], x0,
+                                                       y0, z0, small_types);
     }
     __syncthreads();
     if (tid == 0) {
@@ -593,12 +600,33 @@ __device__ __forceinline__ uint32_t wait_parity(unsigned long long *bar, uint32_
     return done;
 }
 
+// Tally rotation for the next pass, spread over the whole grid: no thread of
+// this pass reads what is written here (engine.h).
+template <int DIM>
+__device__ __forceinline__ void rotate_tallies(const SweepLaunch &a) {
+    constexpr int NM = DIM == 2 ? 5 : 9;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x; l < (size_t)a.n_labels; l += stride) {
+        int dv, ds;
+        unpack_delta(a.vs_prev[l], dv, ds);
+        const int2 b = a.vs_base[l];
+        a.vs_next_base[l] = make_int2(b.x + dv, b.y + ds);
+        a.vs_clear[l] = 0;
+        if (a.tracks) {
+#pragma unroll
+            for (int k = 0; k < NM; ++k) {
+                a.mom_next_base[l * NM + k] = a.mom_base[l * NM + k] + a.mom_prev[l * NM + k];
+                a.mom_clear[l * NM + k] = 0;
+            }
+        }
+    }
+}
+
 template <int DIM, int NOFF, bool UNIFORM>
 __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(const __grid_constant__ SweepLaunch a,
                                                          const __grid_constant__ CUtensorMap tmap) {
     using T = Tile<DIM>;
     using Smem = SweepSmem<DIM>;
-    constexpr int NM = DIM == 2 ? 5 : 9;
     static_assert(Smem::WIN_STRIDE * sizeof(uint32_t) % 128 == 0, "window buffers must stay 128-byte aligned");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // The launch asks for 128 spare bytes so the layout can start on a
@@ -606,32 +634,14 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
     const uint32_t raw = smem_addr(smem_raw);
     Smem &S = *reinterpret_cast<Smem *>(smem_raw + ((128u - (raw & 127u)) & 127u));
 
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     if (smem_addr(S.win[0]) & 127u) {  // never true by construction; refuse rather than copy misaligned
         if (tid == 0) atomicExch(a.error_flag, 3);
         return;
     }
     const int W = a.g.w, H = a.g.h, D = a.g.d;
 
-    // Tally rotation for the next pass: no thread of this pass reads what is
-    // written here (engine.h).
-    {
-        const size_t stride = (size_t)gridDim.x * blockDim.x;
-        for (size_t l = (size_t)blockIdx.x * blockDim.x + tid; l < (size_t)a.n_labels; l += stride) {
-            int dv, ds;
-            unpack_delta(a.vs_prev[l], dv, ds);
-            const int2 b = a.vs_base[l];
-            a.vs_next_base[l] = make_int2(b.x + dv, b.y + ds);
-            a.vs_clear[l] = 0;
-            if (a.tracks) {
-#pragma unroll
-                for (int k = 0; k < NM; ++k) {
-                    a.mom_next_base[l * NM + k] = a.mom_base[l * NM + k] + a.mom_prev[l * NM + k];
-                    a.mom_clear[l * NM + k] = 0;
-                }
-            }
-        }
-    }
+    rotate_tallies<DIM>(a);
 
     const bool small_types = a.n_types <= kSmemTypes;
     if (small_types)
@@ -693,12 +703,265 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
     }
 }
 
+// ---------------------------------------------------------------- the lean sweep
+//
+// Models whose copies price only contact, volume and surface terms (no
+// length, chemotaxis, connectivity veto or moment tracking) take this kernel:
+// the same draws, copies and commits as sweep_kernel, with the work laid out
+// so that no CTA-wide barrier stands between tiles.
+//   - Each warp owns a fixed share of every tile's targets (two rows of them
+//     in a plane) and prices it alone: light pass, its own queue, heavy pass.
+//     Warps drift apart by up to the depth of the window ring.
+//   - Windows arrive through a ring of kLeanStages buffers, by tensor copies
+//     issued up to kLeanStages tiles ahead; the last warp to finish with a
+//     buffer issues the next copy into it.
+//   - A tile on the periodic edge takes the copy with its out-of-lattice
+//     cells filled, then the warps overwrite those cells with the wrapped
+//     labels, each a disjoint share of window rows, and meet on an mbarrier
+//     (a bounded wait) before pricing. Without tensor copies (rows that are
+//     not whole 16-byte units, or a lattice smaller than a window) every cell
+//     of every window is loaded that way.
+constexpr int kLeanStages = 3;
+
+template <int DIM>
+struct LeanSmem {
+    static constexpr int WIN = SweepSmem<DIM>::WIN;
+    static constexpr int WIN_STRIDE = SweepSmem<DIM>::WIN_STRIDE;
+    static constexpr int TPW = Tile<DIM>::NT / kWarps;  // targets per warp per tile
+    alignas(128) uint32_t win[kLeanStages][WIN_STRIDE];
+    uint32_t queue[kWarps][TPW];
+    float contact[kSmemTypes * kSmemTypes];
+    int woff[26];
+    int done[kLeanStages];    // warps finished with the buffer's current tile
+    int issued[kLeanStages];  // copies issued into the buffer
+    alignas(8) unsigned long long full[kLeanStages];     // the buffer's copy has landed
+    alignas(8) unsigned long long patched[kLeanStages];  // every warp has patched its rows
+};
+
+// Tensor copies for every tile, edge tiles included: the lattice's rows are
+// whole 16-byte units and the lattice is at least a window on every axis, so
+// an edge window wraps at most once per axis.
+template <int DIM>
+__device__ __forceinline__ bool lean_copies(const SweepLaunch &a) {
+    using T = Tile<DIM>;
+    return a.use_tma && a.g.w >= T::PX && a.g.h >= T::PY && (DIM == 2 || a.g.d >= T::PZ);
+}
+
+// Start tile i of this CTA's list into its buffer: a tensor copy, or a bare
+// arrival when copies are off, so the buffer's phase completes either way.
+template <int DIM>
+__device__ __forceinline__ void lean_issue(const SweepLaunch &a, const CUtensorMap &tmap, LeanSmem<DIM> &S, int i,
+                                           bool copies) {
+    const int slot = i % kLeanStages;
+    S.issued[slot] += 1;
+    if (copies) {
+        int x0, y0, z0;
+        tile_origin<DIM>((int)blockIdx.x + i * (int)gridDim.x, a.g.w, a.g.h, x0, y0, z0);
+        issue_window<DIM>(tmap, S.win[slot], &S.full[slot], x0, y0, z0);
+    } else {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&S.full[slot])) : "memory");
+    }
+}
+
+// The warp's rows of an edge tile's window (rows warp, warp + kWarps, ...):
+// in a row whose y (and z) lie in the lattice only the cells the copy left
+// filled, else every cell, from the wrapped labels.
+template <int DIM>
+__device__ __forceinline__ void lean_patch(const SweepLaunch &a, uint32_t *win, int x0, int y0, int z0, bool copies) {
+    using T = Tile<DIM>;
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int lo = 0, hi = 0;  // window columns [lo, hi) lie inside the lattice
+    if (copies) {
+        lo = T::HX - x0 > 0 ? T::HX - x0 : 0;
+        hi = W - x0 + T::HX < T::PX ? W - x0 + T::HX : T::PX;
+    }
+    for (int r = warp; r < T::PY * T::PZ; r += kWarps) {
+        const int py = r % T::PY, pz = r / T::PY;
+        const int gy = y0 - 1 + py, gz = DIM == 3 ? z0 - T::HZ + pz : 0;
+        const bool inside = copies && gy >= 0 && gy < H && gz >= 0 && gz < D;
+        const uint32_t *row = a.labels + ((size_t)(DIM == 3 ? wrap(gz, D) : 0) * H + wrap(gy, H)) * W;
+        uint32_t *dst = win + r * T::PX;
+        const int n = inside ? lo + (T::PX - hi) : T::PX;
+        for (int c = lane; c < n; c += 32) {
+            const int px = inside && c >= lo ? hi + (c - lo) : c;
+            dst[px] = row[wrap(x0 - T::HX + px, W)];
+        }
+    }
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+__global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
+    lean_sweep_kernel(const __grid_constant__ SweepLaunch a, const __grid_constant__ CUtensorMap tmap) {
+    using T = Tile<DIM>;
+    using Smem = LeanSmem<DIM>;
+    constexpr int PER_LANE = Smem::TPW / 32;
+    static_assert(Smem::TPW % 32 == 0, "a warp's targets fill whole lanes");
+    static_assert(Smem::WIN_STRIDE * sizeof(uint32_t) % 128 == 0, "window buffers must stay 128-byte aligned");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    Smem &S = *reinterpret_cast<Smem *>(smem_raw + ((128u - (raw & 127u)) & 127u));
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (smem_addr(S.win[0]) & 127u) {  // never true by construction; refuse rather than copy misaligned
+        if (tid == 0) atomicExch(a.error_flag, 3);
+        return;
+    }
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    const int tiles = ((W + T::TX - 1) / T::TX) * ((H + T::TY - 1) / T::TY) * (DIM == 3 ? (D + T::TZ - 1) / T::TZ : 1);
+    const int mine = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const bool copies = lean_copies<DIM>(a);
+
+    if (tid == 0) {
+        for (int k = 0; k < kLeanStages; ++k) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.full[k])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&S.patched[k])), "r"(kWarps));
+            S.done[k] = 0;
+            S.issued[k] = 0;
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int i = 0; i < kLeanStages && i < mine; ++i) lean_issue<DIM>(a, tmap, S, i, copies);
+    }
+    // the rotation's loads overlap the first copies
+    rotate_tallies<DIM>(a);
+    const bool small_types = a.n_types <= kSmemTypes;
+    if (!UNIFORM && small_types)
+        for (int k = tid; k < a.n_types * a.n_types; k += blockDim.x) S.contact[k] = a.t.contact[k];
+#pragma unroll
+    for (int k = 0; k < NOFF; ++k)
+        if (tid == k) S.woff[k] = window_offset<DIM, NOFF>(k);
+    __syncthreads();
+
+    // this lane's targets: offset from the tile's first site, window cell
+    int rel[PER_LANE], cell[PER_LANE];
+#pragma unroll
+    for (int k = 0; k < PER_LANE; ++k) {
+        int lx, ly, lz;
+        target_of<DIM>(warp * Smem::TPW + k * 32 + lane, a.colour, lx, ly, lz);
+        rel[k] = (lz * H + ly) * W + lx;
+        cell[k] = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
+    }
+    uint32_t *queue = S.queue[warp];
+    const unsigned below = (1u << lane) - 1u;
+    uint32_t patch_parity = 0;  // bit k: parity of the next phase of patched[k]
+
+    for (int i = 0; i < mine; ++i) {
+        const int slot = i % kLeanStages;
+        int x0, y0, z0;
+        tile_origin<DIM>((int)blockIdx.x + i * (int)gridDim.x, W, H, x0, y0, z0);
+        uint32_t *win = S.win[slot];
+        bool ok = wait_parity(&S.full[slot], (uint32_t)(i / kLeanStages) & 1u) != 0;
+        const bool edge = !copies || !(x0 >= T::HX && x0 + T::TX + T::HX <= W && y0 >= 1 && y0 + T::TY + 1 <= H &&
+                                       (DIM == 2 || (z0 >= 1 && z0 + T::TZ + 1 <= D)));
+        if (edge && __all_sync(0xffffffffu, ok)) {
+            lean_patch<DIM>(a, win, x0, y0, z0, copies);
+            // generic writes to a buffer a later tensor copy will overwrite
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&S.patched[slot])) : "memory");
+            ok = wait_parity(&S.patched[slot], (patch_parity >> slot) & 1u) != 0;
+            patch_parity ^= 1u << slot;
+        }
+        if (!__all_sync(0xffffffffu, ok)) {
+            // A copy or a warp that never came: flag it, give each buffer's
+            // latest copy its own bounded wait so none lands after exit, stop.
+            if (lane == 0) {
+                atomicExch(a.error_flag, 1);
+                for (int k = 0; k < kLeanStages; ++k)
+                    if (S.issued[k] > 0) wait_parity(&S.full[k], (uint32_t)(S.issued[k] - 1) & 1u);
+            }
+            return;
+        }
+
+        // Light pass: this warp's targets; those whose neighbour pick carries
+        // another label go into the warp's queue.
+        const bool full = x0 + T::TX <= W && y0 + T::TY <= H && (DIM == 2 || z0 + T::TZ <= D);
+        const uint32_t tile_base = (uint32_t)((z0 * H + y0) * W + x0);
+        uint32_t entries[PER_LANE];
+        unsigned masks[PER_LANE];
+#pragma unroll
+        for (int k = 0; k < PER_LANE; ++k) {
+            const int j = warp * Smem::TPW + k * 32 + lane;
+            bool in = full;
+            if (!full) {
+                int lx, ly, lz;
+                target_of<DIM>(j, a.colour, lx, ly, lz);
+                in = x0 + lx < W && y0 + ly < H && (DIM == 2 || z0 + lz < D);
+            }
+            bool active = false;
+            int pick = 0;
+            if (in) {
+                pick = (int)(draw(a.key_pick, tile_base + (uint32_t)rel[k]) % (uint64_t)NOFF);
+                active = win[cell[k]] != win[cell[k] + S.woff[pick]];
+            }
+            entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
+            masks[k] = __ballot_sync(0xffffffffu, active);
+        }
+        int queued = 0;
+#pragma unroll
+        for (int k = 0; k < PER_LANE; ++k) {
+            if (masks[k] & (1u << lane)) queue[queued + __popc(masks[k] & below)] = entries[k];
+            queued += __popc(masks[k]);
+        }
+        __syncwarp();
+        // Heavy pass: the queue, 32 copies at a time.
+        for (int b = 0; b < queued; b += 32)
+            if (b + lane < queued)
+                price_and_commit<DIM, NOFF, UNIFORM, false>(a, S.woff, S.contact, nullptr, win, queue[b + lane], x0,
+                                                            y0, z0, small_types);
+        __syncwarp();
+
+        // Done with the buffer; the last warp out refills it.
+        if (lane == 0) {
+            __threadfence_block();
+            if (atomicAdd(&S.done[slot], 1) == kWarps - 1) {
+                S.done[slot] = 0;
+                if (i + kLeanStages < mine) {
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    lean_issue<DIM>(a, tmap, S, i + kLeanStages, copies);
+                }
+            }
+        }
+    }
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cudaStream_t stream) {
+    using T = Tile<DIM>;
+    static int grid_cap = 0;
+    const size_t smem = sizeof(LeanSmem<DIM>) + 128;
+    if (!grid_cap) {
+        cudaError_t e = cudaFuncSetAttribute(lean_sweep_kernel<DIM, NOFF, UNIFORM>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e) return e;
+        int dev = 0, sms = 0, per_sm = 0;
+        if ((e = cudaGetDevice(&dev))) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lean_sweep_kernel<DIM, NOFF, UNIFORM>,
+                                                               kThreads, smem)))
+            return e;
+        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    const int tiles = ((a.g.w + T::TX - 1) / T::TX) * ((a.g.h + T::TY - 1) / T::TY) *
+                      (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
+    int grid = tiles < grid_cap ? tiles : grid_cap;
+    if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
+    lean_sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kThreads, smem, stream>>>(a, tmap);
+    return cudaGetLastError();
+}
+
 template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
     // the compile-time neighbourhood must be the one the host built
     for (int k = 0; k < NOFF; ++k)
         for (int axis = 0; axis < 3; ++axis)
             if (a.g.off[k][axis] != neighbour_offset<DIM, NOFF>(k, axis)) return cudaErrorInvalidValue;
+    CUtensorMap tmap;
+    if (a.use_tma && a.tensor_map)
+        tmap = *static_cast<const CUtensorMap *>(a.tensor_map);
+    else
+        memset(&tmap, 0, sizeof tmap);
+    if (a.lean) return launch_lean<DIM, NOFF, UNIFORM>(a, tmap, stream);
     using T = Tile<DIM>;
     static int grid_cap = 0;
     const size_t smem = sizeof(SweepSmem<DIM>) + 128;
@@ -717,11 +980,6 @@ static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
                       (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
     int grid = tiles < grid_cap ? tiles : grid_cap;
     if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
-    CUtensorMap tmap;
-    if (a.use_tma && a.tensor_map)
-        tmap = *static_cast<const CUtensorMap *>(a.tensor_map);
-    else
-        memset(&tmap, 0, sizeof tmap);
     sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kThreads, smem, stream>>>(a, tmap);
     return cudaGetLastError();
 }

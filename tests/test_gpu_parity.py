@@ -3,9 +3,11 @@
 Every case runs the same start on the B200 (through the C ABI) and on the
 replay (oracle/replay.c) and requires identical labels, per-label volumes,
 surfaces and cell types, and bit-identical f32 fields. Each case runs with
-the sweep's tensor-copy window load on and off, and with the persistent grid
-at its default and capped at three CTAs (each CTA then walks several tiles
-through both window buffers), so every load path is held to one result.
+the sweep's tensor-copy window load on and off, with the persistent grid at
+its default and capped at three CTAs (each CTA then walks several tiles
+through every window buffer), and on both sweep kernels (the lean one takes
+the models that price contact, volume and surface only; the general one
+every model), so every load path and both kernels are held to one result.
 """
 
 from __future__ import annotations
@@ -40,6 +42,21 @@ def _large():
     m = sheet_model(width=384, height=192, seed=2, contact=(0, 10, 10, 10), lambda_volume=1.0,
                     target_surface=92.0, lambda_surface=0.2)
     return tiled(m), 10
+
+
+def _ragged():
+    # 264 x 180: tiles overhang the right and bottom edges, and edge windows
+    # take a tensor copy with out-of-lattice cells filled, then patched
+    m = sheet_model(width=264, height=180, seed=9, contact=(0, 10, 10, 10), lambda_volume=1.0,
+                    target_surface=92.0, lambda_surface=0.2)
+    return tiled(m), 8
+
+
+def _ragged_volume():
+    # 152 x 24 x 20: overhanging tiles on x and z, edge windows copied and patched
+    m = sheet_model(width=152, height=24, depth=20, seed=10, target_volume=512.0, order=3,
+                    contact=(0, 10, 10, 10), lambda_volume=1.0)
+    return tiled(m), 3
 
 
 def _unaligned():
@@ -109,6 +126,8 @@ CASES = {
     "surface": _surface,
     "von-neumann": _von_neumann,
     "large": _large,
+    "ragged": _ragged,
+    "ragged-volume": _ragged_volume,
     "unaligned": _unaligned,
     "medium": _medium,
     "volume-26": _volume(3),
@@ -124,16 +143,19 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("lean", ["1", "0"])
 @pytest.mark.parametrize("ctas", ["0", "3"])
 @pytest.mark.parametrize("tma", ["1", "0"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, monkeypatch):
+def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, lean, monkeypatch):
     """`ctas` 3 caps the sweep's persistent grid at three CTAs, so every CTA
-    walks several tiles and both window buffers take tensor copies."""
+    walks several tiles and every window buffer takes tensor copies; `lean` 0
+    keeps the model on the general kernel."""
     made, steps = CASES[name]()
     start, fields = made if isinstance(made, tuple) else (made, None)
     monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
     monkeypatch.setenv("GLAZIER_SWEEP_CTAS", ctas)
+    monkeypatch.setenv("GLAZIER_SWEEP_LEAN", lean)
     gpu = device.GpuSimulation.from_start(start, fields)
     replay = ReplayOracle.from_start(start, fields)
     for chunk in (1, steps - 1):
