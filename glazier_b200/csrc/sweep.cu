@@ -430,9 +430,13 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const int
     if (EXTRAS && (a.has_length || a.has_chemotaxis))
         delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
 
-    if (delta > 0.0f) {
+    // Metropolis: a copy that lowers the energy (or keeps it) is taken, else
+    // with probability exp(-delta / T). The draw and the exponential are
+    // computed on every lane, so the test needs no branch; a lane whose delta
+    // is not positive takes the copy whatever they say.
+    {
         const float u = to_f32(draw(a.key_accept, target));
-        if (!(u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
+        if (!(delta <= 0.0f || u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
     }
 
     a.labels[target] = nw;
@@ -729,7 +733,7 @@ struct LeanSmem {
     static constexpr int WIN_STRIDE = SweepSmem<DIM>::WIN_STRIDE;
     static constexpr int TPW = Tile<DIM>::NT / kWarps;  // targets per warp per tile
     alignas(128) uint32_t win[kLeanStages][WIN_STRIDE];
-    uint32_t queue[kWarps][TPW];
+    uint32_t queue[kWarps][TPW + 32];  // a tile's entries after fewer than 32 held from the tile before
     float contact[kSmemTypes * kSmemTypes];
     int woff[26];
     int done[kLeanStages];    // warps finished with the buffer's current tile
@@ -790,6 +794,23 @@ __device__ __forceinline__ void lean_patch(const SweepLaunch &a, uint32_t *win, 
     }
 }
 
+// The warp is done with tile i's buffer (lane 0 acts); the last warp out
+// refills it with tile i + kLeanStages.
+template <int DIM>
+__device__ __forceinline__ void lean_release(const SweepLaunch &a, const CUtensorMap &tmap, LeanSmem<DIM> &S, int i,
+                                             int mine, bool copies) {
+    if ((threadIdx.x & 31) != 0) return;
+    const int slot = i % kLeanStages;
+    __threadfence_block();
+    if (atomicAdd(&S.done[slot], 1) == kWarps - 1) {
+        S.done[slot] = 0;
+        if (i + kLeanStages < mine) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            lean_issue<DIM>(a, tmap, S, i + kLeanStages, copies);
+        }
+    }
+}
+
 template <int DIM, int NOFF, bool UNIFORM>
 __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
     lean_sweep_kernel(const __grid_constant__ SweepLaunch a, const __grid_constant__ CUtensorMap tmap) {
@@ -843,11 +864,28 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
     uint32_t *queue = S.queue[warp];
     const unsigned below = (1u << lane) - 1u;
     uint32_t patch_parity = 0;  // bit k: parity of the next phase of patched[k]
+    // entries held over from the previous tile: queue[0, held), its buffer and origin
+    int held = 0, held_slot = -1, hx0 = 0, hy0 = 0, hz0 = 0;
+    // The CTA's tiles are blockIdx.x + i gridDim.x; their tile coordinates
+    // advance by the grid's own decomposition, so the loop divides nothing.
+    const int tiles_x = (W + T::TX - 1) / T::TX, tiles_y = (H + T::TY - 1) / T::TY;
+    const int step_x = (int)gridDim.x % tiles_x, step_y = ((int)gridDim.x / tiles_x) % tiles_y;
+    const int step_z = (int)gridDim.x / (tiles_x * tiles_y);
+    int tx = (int)blockIdx.x % tiles_x, ty = ((int)blockIdx.x / tiles_x) % tiles_y;
+    int tz = (int)blockIdx.x / (tiles_x * tiles_y);
 
     for (int i = 0; i < mine; ++i) {
         const int slot = i % kLeanStages;
-        int x0, y0, z0;
-        tile_origin<DIM>((int)blockIdx.x + i * (int)gridDim.x, W, H, x0, y0, z0);
+        if (i > 0) {
+            tx += step_x;
+            const int cx = tx >= tiles_x;
+            tx -= cx ? tiles_x : 0;
+            ty += step_y + cx;
+            const int cy = ty >= tiles_y;
+            ty -= cy ? tiles_y : 0;
+            tz += step_z + cy;
+        }
+        const int x0 = tx * T::TX, y0 = ty * T::TY, z0 = DIM == 3 ? tz * T::TZ : 0;
         uint32_t *win = S.win[slot];
         bool ok = wait_parity(&S.full[slot], (uint32_t)(i / kLeanStages) & 1u) != 0;
         const bool edge = !copies || !(x0 >= T::HX && x0 + T::TX + T::HX <= W && y0 >= 1 && y0 + T::TY + 1 <= H &&
@@ -874,7 +912,8 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
         }
 
         // Light pass: this warp's targets; those whose neighbour pick carries
-        // another label go into the warp's queue.
+        // another label go into the warp's queue, behind the entries held
+        // from the previous tile.
         const bool full = x0 + T::TX <= W && y0 + T::TY <= H && (DIM == 2 || z0 + T::TZ <= D);
         const uint32_t tile_base = (uint32_t)((z0 * H + y0) * W + x0);
         uint32_t entries[PER_LANE];
@@ -897,31 +936,55 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
             entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
             masks[k] = __ballot_sync(0xffffffffu, active);
         }
-        int queued = 0;
+        int total = held;
 #pragma unroll
         for (int k = 0; k < PER_LANE; ++k) {
-            if (masks[k] & (1u << lane)) queue[queued + __popc(masks[k] & below)] = entries[k];
-            queued += __popc(masks[k]);
+            if (masks[k] & (1u << lane)) queue[total + __popc(masks[k] & below)] = entries[k];
+            total += __popc(masks[k]);
         }
         __syncwarp();
-        // Heavy pass: the queue, 32 copies at a time.
-        for (int b = 0; b < queued; b += 32)
-            if (b + lane < queued)
-                price_and_commit<DIM, NOFF, UNIFORM, false>(a, S.woff, S.contact, nullptr, win, queue[b + lane], x0,
-                                                            y0, z0, small_types);
-        __syncwarp();
-
-        // Done with the buffer; the last warp out refills it.
-        if (lane == 0) {
-            __threadfence_block();
-            if (atomicAdd(&S.done[slot], 1) == kWarps - 1) {
-                S.done[slot] = 0;
-                if (i + kLeanStages < mine) {
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    lean_issue<DIM>(a, tmap, S, i + kLeanStages, copies);
-                }
+        // Heavy pass: whole rounds of 32 copies, oldest first; entry e is the
+        // previous tile's when e < held. Whatever of the previous tile is still
+        // queued after them goes in one last short round, so that tile's
+        // buffer can be let go; fewer than 32 of this tile's stay held.
+        int taken = 0;
+        for (;;) {
+            const int n = total - taken;
+            if (n < 32 && taken >= held) break;
+            const int e = taken + lane;
+            if (e < total) {
+                const bool before = e < held;
+                price_and_commit<DIM, NOFF, UNIFORM, false>(a, S.woff, S.contact, nullptr,
+                                                            before ? S.win[held_slot] : win, queue[e],
+                                                            before ? hx0 : x0, before ? hy0 : y0,
+                                                            before ? hz0 : z0, small_types);
             }
+            taken += n < 32 ? n : 32;
         }
+        __syncwarp();
+        if (held_slot >= 0) lean_release<DIM>(a, tmap, S, i - 1, mine, copies);
+        // move what this tile keeps to the front of the queue (a full round
+        // came first, so the source lies past the first 32 entries)
+        const int keep = total - taken;
+        if (taken > 0 && keep > 0) {
+            const uint32_t v = lane < keep ? queue[taken + lane] : 0u;
+            __syncwarp();
+            if (lane < keep) queue[lane] = v;
+            __syncwarp();
+        }
+        held = keep;
+        held_slot = slot;
+        hx0 = x0;
+        hy0 = y0;
+        hz0 = z0;
+    }
+    // the last tile's held entries, then its buffer
+    if (mine > 0) {
+        if (lane < held)
+            price_and_commit<DIM, NOFF, UNIFORM, false>(a, S.woff, S.contact, nullptr, S.win[held_slot], queue[lane],
+                                                        hx0, hy0, hz0, small_types);
+        __syncwarp();
+        lean_release<DIM>(a, tmap, S, mine - 1, mine, copies);
     }
 }
 
