@@ -136,7 +136,7 @@ def measured_peak() -> tuple:
 
 def committed_traffic():
     """DRAM bytes per sweep launch from the committed ncu summary, if any."""
-    path = ROOT / "profiles" / "sweep_2d_4096.md"
+    path = ROOT / "profiles" / "lean_sweep_2d_4096.md"
     if not path.exists():
         return None
     for line in path.read_text().splitlines():
@@ -390,7 +390,7 @@ def run_ours(args) -> None:
     achieved = bytes_per_launch / launch_s / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": committed_traffic(), "peak_source": peak_kind,
-                "kernel": "sweep_kernel<2,8> (one colour pass)",
+                "kernel": "lean_sweep_kernel<2,8,1> (one colour pass)",
                 "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3}
 
     sim.close()
@@ -402,7 +402,7 @@ def run_ours(args) -> None:
     line = {
         "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": value / world / PUBLISHED_4096, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": value / PUBLISHED_4096, "dtype": "f32", "data": "synthetic",
         "config": config_dict(args.size, world),
         "e2e": {"value": e2e_value, "unit": "site-updates/s", "h2d_bytes_per_step": sites * 4,
                 "d2h_bytes_per_step": sites * 4, "jobs": jobs, "mcs_per_job": job_mcs},
