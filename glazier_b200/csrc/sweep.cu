@@ -28,6 +28,7 @@
 
 #include "device.cuh"
 #include "engine.h"
+#include "neighbours.cuh"
 
 namespace glz {
 
@@ -51,36 +52,6 @@ struct Tile<3> {
     static constexpr int HZ = 1;
     static constexpr int NT = (TX / 2) * (TY / 2) * (TZ / 2);
 };
-
-// The neighbour offsets of each neighbourhood in the reference's order
-// (lattice.rs:8-88): a plane takes ORDER1's four in-plane faces or ORDER3's
-// eight in-plane neighbours; a volume takes ORDER1, ORDER2 or ORDER3 whole.
-// The host builds the same table (engine.cu) and the launch checks they agree.
-template <int DIM, int NOFF>
-__host__ __device__ constexpr int neighbour_offset(int k, int axis) {
-    if (DIM == 2 && NOFF == 4) {
-        constexpr int o[4][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}};
-        return o[k][axis];
-    }
-    if (DIM == 2 && NOFF == 8) {
-        constexpr int o[8][3] = {{-1, -1, 0}, {0, -1, 0}, {1, -1, 0}, {-1, 0, 0},
-                                 {1, 0, 0},   {-1, 1, 0}, {0, 1, 0},  {1, 1, 0}};
-        return o[k][axis];
-    }
-    if (DIM == 3 && NOFF == 6) {
-        constexpr int o[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
-        return o[k][axis];
-    }
-    if (DIM == 3 && NOFF == 18) {
-        constexpr int o[18][3] = {{1, 0, 0},  {-1, 0, 0}, {0, 1, 0},   {0, -1, 0}, {0, 0, 1},  {0, 0, -1},
-                                  {1, 1, 0},  {1, -1, 0}, {-1, 1, 0},  {-1, -1, 0}, {1, 0, 1}, {1, 0, -1},
-                                  {-1, 0, 1}, {-1, 0, -1}, {0, 1, 1}, {0, 1, -1}, {0, -1, 1}, {0, -1, -1}};
-        return o[k][axis];
-    }
-    // ORDER3: dz, then dy, then dx from -1 to 1, the centre left out
-    const int kk = k < 13 ? k : k + 1;
-    return axis == 0 ? kk % 3 - 1 : (axis == 1 ? (kk / 3) % 3 - 1 : kk / 9 - 1);
-}
 
 template <int DIM, int NOFF>
 __host__ __device__ constexpr int window_offset(int k) {
@@ -726,14 +697,22 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
 //     not whole 16-byte units, or a lattice smaller than a window) every cell
 //     of every window is loaded that way.
 constexpr int kLeanStages = 3;
+#ifndef GLZ_LEAN_WARPS
+#define GLZ_LEAN_WARPS 8
+#endif
+#ifndef GLZ_LEAN_MIN_BLOCKS
+#define GLZ_LEAN_MIN_BLOCKS 3
+#endif
+constexpr int kLeanWarps = GLZ_LEAN_WARPS;
+constexpr int kLeanThreads = 32 * kLeanWarps;
 
 template <int DIM>
 struct LeanSmem {
     static constexpr int WIN = SweepSmem<DIM>::WIN;
     static constexpr int WIN_STRIDE = SweepSmem<DIM>::WIN_STRIDE;
-    static constexpr int TPW = Tile<DIM>::NT / kWarps;  // targets per warp per tile
+    static constexpr int TPW = Tile<DIM>::NT / kLeanWarps;  // targets per warp per tile
     alignas(128) uint32_t win[kLeanStages][WIN_STRIDE];
-    uint32_t queue[kWarps][TPW + 32];  // a tile's entries after fewer than 32 held from the tile before
+    uint32_t queue[kLeanWarps][TPW + 32];  // a tile's entries after fewer than 32 held from the tile before
     float contact[kSmemTypes * kSmemTypes];
     int woff[26];
     int done[kLeanStages];    // warps finished with the buffer's current tile
@@ -767,7 +746,7 @@ __device__ __forceinline__ void lean_issue(const SweepLaunch &a, const CUtensorM
     }
 }
 
-// The warp's rows of an edge tile's window (rows warp, warp + kWarps, ...):
+// The warp's rows of an edge tile's window (rows warp, warp + kLeanWarps, ...):
 // in a row whose y (and z) lie in the lattice only the cells the copy left
 // filled, else every cell, from the wrapped labels.
 template <int DIM>
@@ -780,7 +759,7 @@ __device__ __forceinline__ void lean_patch(const SweepLaunch &a, uint32_t *win, 
         lo = T::HX - x0 > 0 ? T::HX - x0 : 0;
         hi = W - x0 + T::HX < T::PX ? W - x0 + T::HX : T::PX;
     }
-    for (int r = warp; r < T::PY * T::PZ; r += kWarps) {
+    for (int r = warp; r < T::PY * T::PZ; r += kLeanWarps) {
         const int py = r % T::PY, pz = r / T::PY;
         const int gy = y0 - 1 + py, gz = DIM == 3 ? z0 - T::HZ + pz : 0;
         const bool inside = copies && gy >= 0 && gy < H && gz >= 0 && gz < D;
@@ -802,7 +781,7 @@ __device__ __forceinline__ void lean_release(const SweepLaunch &a, const CUtenso
     if ((threadIdx.x & 31) != 0) return;
     const int slot = i % kLeanStages;
     __threadfence_block();
-    if (atomicAdd(&S.done[slot], 1) == kWarps - 1) {
+    if (atomicAdd(&S.done[slot], 1) == kLeanWarps - 1) {
         S.done[slot] = 0;
         if (i + kLeanStages < mine) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -812,7 +791,7 @@ __device__ __forceinline__ void lean_release(const SweepLaunch &a, const CUtenso
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
-__global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
+__global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
     lean_sweep_kernel(const __grid_constant__ SweepLaunch a, const __grid_constant__ CUtensorMap tmap) {
     using T = Tile<DIM>;
     using Smem = LeanSmem<DIM>;
@@ -835,7 +814,7 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
     if (tid == 0) {
         for (int k = 0; k < kLeanStages; ++k) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.full[k])));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&S.patched[k])), "r"(kWarps));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&S.patched[k])), "r"(kLeanWarps));
             S.done[k] = 0;
             S.issued[k] = 0;
         }
@@ -1001,7 +980,7 @@ static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cu
         if ((e = cudaGetDevice(&dev))) return e;
         if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lean_sweep_kernel<DIM, NOFF, UNIFORM>,
-                                                               kThreads, smem)))
+                                                               kLeanThreads, smem)))
             return e;
         grid_cap = sms * (per_sm > 0 ? per_sm : 1);
     }
@@ -1009,7 +988,7 @@ static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cu
                       (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
     int grid = tiles < grid_cap ? tiles : grid_cap;
     if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
-    lean_sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kThreads, smem, stream>>>(a, tmap);
+    lean_sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kLeanThreads, smem, stream>>>(a, tmap);
     return cudaGetLastError();
 }
 

@@ -12,13 +12,17 @@
 
 #include "device.cuh"
 #include "engine.h"
+#include "neighbours.cuh"
 
 namespace glz {
 
+// A lattice holds fewer than 2^31 sites, so 32-bit division suffices.
 __device__ __forceinline__ void coords_of(const Geometry &g, size_t i, int &x, int &y, int &z) {
-    x = (int)(i % g.w);
-    y = (int)((i / g.w) % g.h);
-    z = (int)(i / ((size_t)g.w * g.h));
+    const uint32_t s = (uint32_t)i, w = (uint32_t)g.w, h = (uint32_t)g.h;
+    const uint32_t row = s / w;
+    x = (int)(s - row * w);
+    y = (int)(row % h);
+    z = (int)(row / h);
 }
 
 __global__ void fill_anchor_kernel(int *anchor, int n) {
@@ -30,27 +34,118 @@ __global__ void fill_anchor_kernel(int *anchor, int n) {
     anchor[4 * l + 3] = INT_MAX;
 }
 
-__global__ void recount_counts_kernel(const __grid_constant__ RecountLaunch a) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)a.g.sites) return;
-    const uint32_t l = a.labels[i];
-    if (l >= (uint32_t)a.n_labels) {
-        atomicExch(a.error_flag, 2);
-        return;
-    }
-    int x, y, z;
-    coords_of(a.g, i, x, y, z);
+// Unlike-label neighbours of site i (label l) at (x, y, z), in 32-bit index
+// arithmetic: the wrapped coordinates one step either side are formed once
+// and each offset picks among them. A neighbour that wraps onto the site
+// itself is not a bond.
+__device__ __forceinline__ int unlike_neighbours(const Geometry &g, const uint32_t *labels, uint32_t i, uint32_t l,
+                                                 int x, int y, int z) {
+    const int W = g.w, H = g.h, D = g.d;
+    const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
+    const int zm = z == 0 ? D - 1 : z - 1, zp = z == D - 1 ? 0 : z + 1;
     int bonds = 0;
-    for (int k = 0; k < a.g.n_off; ++k) {
-        const size_t n = ((size_t)wrap(z + a.g.off[k][2], a.g.d) * a.g.h + wrap(y + a.g.off[k][1], a.g.h)) * a.g.w +
-                         wrap(x + a.g.off[k][0], a.g.w);
-        if (n != i && a.labels[n] != l) ++bonds;
+    for (int k = 0; k < g.n_off; ++k) {
+        const int dx = g.off[k][0], dy = g.off[k][1], dz = g.off[k][2];
+        const uint32_t nx = (uint32_t)(dx < 0 ? xm : (dx > 0 ? xp : x));
+        const uint32_t ny = (uint32_t)(dy < 0 ? ym : (dy > 0 ? yp : y));
+        const uint32_t nz = (uint32_t)(dz < 0 ? zm : (dz > 0 ? zp : z));
+        const uint32_t n = (nz * (uint32_t)H + ny) * (uint32_t)W + nx;
+        bonds += n != i && labels[n] != l;
     }
-    const int colour = (x & 1) | ((y & 1) << 1) | (a.g.dim == 3 ? ((z & 1) << 2) : 0);
-    atomicAdd(&a.vs_base[l].x, 1);
-    if (bonds) atomicAdd(&a.vs_base[l].y, bonds);
-    atomicAdd(&a.vol_by_colour[(size_t)l * a.g.ncol + colour], 1);
-    atomicMin(&a.anchor[4 * (size_t)l + 3], (int)i);
+    return bonds;
+}
+
+// Volume, unlike-bond surface, per-colour volume and first site of every
+// label. Blocks run along lattice rows (x across threads, one row per block
+// row), so a warp holds 32 consecutive sites of one row and a cell usually
+// covers a run of lanes: each run adds its counts through its first lane
+// (whose site is also the run's first), one atomic per run, not per site.
+// Along a row only x changes, so a run's sites alternate between two
+// colours, starting with its first lane's. A label that comes back later in
+// the warp starts another run. Neighbour addresses are the compile-time
+// neighbourhood's offsets over the wrapped rows and columns either side.
+template <int DIM, int NOFF>
+__global__ void recount_counts_kernel(const __grid_constant__ RecountLaunch a) {
+    constexpr uint32_t kNone = 0xffffffffu;
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    const int lane = threadIdx.x & 31;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
+    for (int row = blockIdx.y; row < H * D; row += gridDim.y) {
+        const int y = row % H, z = row / H;
+        const uint32_t i = (uint32_t)row * (uint32_t)W + (uint32_t)x;
+        uint32_t l = x < W ? a.labels[i] : kNone;
+        if (l != kNone && l >= (uint32_t)a.n_labels) {
+            atomicExch(a.error_flag, 2);
+            l = kNone;
+        }
+        int bonds = 0;
+        if (l != kNone) {
+            const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
+            const int zm = z == 0 ? D - 1 : z - 1, zp = z == D - 1 ? 0 : z + 1;
+#pragma unroll
+            for (int k = 0; k < NOFF; ++k) {
+                const int dx = neighbour_offset<DIM, NOFF>(k, 0), dy = neighbour_offset<DIM, NOFF>(k, 1),
+                          dz = neighbour_offset<DIM, NOFF>(k, 2);
+                const uint32_t nx = (uint32_t)(dx < 0 ? xm : (dx > 0 ? xp : x));
+                const uint32_t ny = (uint32_t)(dy < 0 ? ym : (dy > 0 ? yp : y));
+                const uint32_t nz = (uint32_t)(dz < 0 ? zm : (dz > 0 ? zp : z));
+                const uint32_t n = (nz * (uint32_t)H + ny) * (uint32_t)W + nx;
+                // a neighbour that wraps onto the site itself is not a bond
+                bonds += n != i && a.labels[n] != l;
+            }
+        }
+        const int colour = (x & 1) | ((y & 1) << 1) | (DIM == 3 ? ((z & 1) << 2) : 0);
+        const unsigned full = 0xffffffffu;
+        const uint32_t before = __shfl_up_sync(full, l, 1);
+        const bool head = lane == 0 || l != before;
+        const unsigned heads = __ballot_sync(full, head);
+        // inclusive prefix sum of the bond counts over the warp
+        int scan = bonds;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(full, scan, o);
+            if (lane >= o) scan += v;
+        }
+        const unsigned later = heads & ~(full >> (31 - lane));  // heads after this lane
+        const int last = later ? __ffs(later) - 2 : 31;          // this lane's run ends here
+        const int scan_last = __shfl_sync(full, scan, last);
+        if (head && l != kNone) {
+            const int len = last - lane + 1;
+            const int run_bonds = scan_last - scan + bonds;
+            atomicAdd(&a.vs_base[l].x, len);
+            if (run_bonds) atomicAdd(&a.vs_base[l].y, run_bonds);
+            atomicMin(&a.anchor[4 * (size_t)l + 3], (int)i);
+            int *by_colour = &a.vol_by_colour[(size_t)l * a.g.ncol];
+            atomicAdd(&by_colour[colour], (len + 1) / 2);
+            if (len > 1) atomicAdd(&by_colour[colour ^ 1], len / 2);
+        }
+    }
+}
+
+template <int DIM, int NOFF>
+static cudaError_t launch_counts(const RecountLaunch &a, cudaStream_t stream) {
+    for (int k = 0; k < NOFF; ++k)
+        for (int axis = 0; axis < 3; ++axis)
+            if (a.g.off[k][axis] != neighbour_offset<DIM, NOFF>(k, axis)) return cudaErrorInvalidValue;
+    const int bx = a.g.w >= 256 ? 256 : (a.g.w + 31) / 32 * 32;
+    const int rows = a.g.h * a.g.d;
+    const dim3 grid((unsigned)((a.g.w + bx - 1) / bx), (unsigned)(rows < 65535 ? rows : 65535));
+    recount_counts_kernel<DIM, NOFF><<<grid, bx, 0, stream>>>(a);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_counts_any(const RecountLaunch &a, cudaStream_t stream) {
+    if (a.g.dim == 2) {
+        if (a.g.n_off == 4) return launch_counts<2, 4>(a, stream);
+        if (a.g.n_off == 8) return launch_counts<2, 8>(a, stream);
+    } else {
+        if (a.g.n_off == 6) return launch_counts<3, 6>(a, stream);
+        if (a.g.n_off == 18) return launch_counts<3, 18>(a, stream);
+        if (a.g.n_off == 26) return launch_counts<3, 26>(a, stream);
+    }
+    return cudaErrorInvalidValue;
 }
 
 __global__ void recount_anchor_kernel(const __grid_constant__ RecountLaunch a) {
@@ -111,7 +206,7 @@ cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream) {
     const int lb = (int)((n + 255) / 256);
     const int sb = (a.g.sites + 255) / 256;
     fill_anchor_kernel<<<lb, 256, 0, stream>>>(a.anchor, (int)n);
-    recount_counts_kernel<<<sb, 256, 0, stream>>>(a);
+    if (cudaError_t e = launch_counts_any(a, stream)) return e;
     recount_anchor_kernel<<<lb, 256, 0, stream>>>(a);
     if (a.tracks) recount_moments_kernel<<<sb, 256, 0, stream>>>(a);
     return cudaGetLastError();
@@ -149,11 +244,7 @@ __global__ void medium_count_kernel(const __grid_constant__ Geometry g, const ui
         int x, y, z;
         coords_of(g, i, x, y, z);
         sites = 1;
-        for (int k = 0; k < g.n_off; ++k) {
-            const size_t n =
-                ((size_t)wrap(z + g.off[k][2], g.d) * g.h + wrap(y + g.off[k][1], g.h)) * g.w + wrap(x + g.off[k][0], g.w);
-            if (n != i && labels[n] != 0) ++bonds;
-        }
+        bonds = (unsigned long long)unlike_neighbours(g, labels, (uint32_t)i, 0u, x, y, z);
     }
     for (int o = 16; o > 0; o >>= 1) {
         sites += __shfl_down_sync(0xffffffffu, sites, o);
