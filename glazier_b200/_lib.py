@@ -118,6 +118,8 @@ def lib():
     for name in ("glz_gpu_volumes", "glz_gpu_surfaces", "glz_gpu_cell_types"):
         getattr(L, name).restype = C.c_int
         getattr(L, name).argtypes = [_P, _P, C.POINTER(C.c_size_t)]
+    L.glz_gpu_set_infection.restype = C.c_int
+    L.glz_gpu_set_infection.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_double]
     L.glz_gpu_set_nematic_field.restype = C.c_int
     L.glz_gpu_set_nematic_field.argtypes = [_P, _P, C.c_size_t]
     L.glz_gpu_mcs.restype = C.c_uint64

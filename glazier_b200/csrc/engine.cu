@@ -133,6 +133,10 @@ struct glz_gpu {
     int max_ctas = 0;
     int uniform = -1;
     bool uniform_exact = false;
+    // the infection rule (glz_gpu_set_infection); dose per label, cap entries
+    int infect_species = -1, infect_from = 0, infect_to = 0;
+    long long infect_threshold = 0;
+    unsigned long long *dose = nullptr;
     float uniform_j = 0.0f;
     std::vector<float> host_tv, host_lv, host_ts, host_ls;
     CUtensorMap tmap{};
@@ -229,8 +233,16 @@ int alloc_labels(glz_gpu *h, size_t cap) {
     if (int rc = dev_alloc(&fresh.anchor, cap * 4)) return rc;
     uint8_t *types = nullptr;
     if (int rc = dev_alloc(&types, cap)) return rc;
-    if (n) CU(cudaMemcpyAsync(types, h->cell_type_host.data(), n, cudaMemcpyHostToDevice, h->stream));
+    unsigned long long *dose = nullptr;
+    if (int rc = dev_alloc(&dose, cap)) return rc;
+    CU(cudaMemsetAsync(dose, 0, cap * sizeof(unsigned long long), h->stream));
+    // the device holds the live types (an infection may have switched some)
+    if (n && h->cap)
+        CU(cudaMemcpyAsync(types, h->cell_type, n, cudaMemcpyDeviceToDevice, h->stream));
+    else if (n)
+        CU(cudaMemcpyAsync(types, h->cell_type_host.data(), n, cudaMemcpyHostToDevice, h->stream));
     if (h->cap) {
+        CU(cudaMemcpyAsync(dose, h->dose, n * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, h->stream));
         // the caller has settled: base slot p % 2 holds every tally
         CU(cudaMemcpyAsync(fresh.vs_base[p % 2], h->t.vs_base[p % 2], n * sizeof(int2), cudaMemcpyDeviceToDevice,
                            h->stream));
@@ -253,6 +265,8 @@ int alloc_labels(glz_gpu *h, size_t cap) {
     }
     cudaFree(h->cell_type);
     h->cell_type = types;
+    cudaFree(h->dose);
+    h->dose = dose;
     h->cap = cap;
     return GLZ_OK;
 }
@@ -369,6 +383,9 @@ int field_step(glz_gpu *h) {
         f.cell_type = h->cell_type;
         f.secretion = h->sec;
         f.uptake = h->upt;
+        f.infect_species = h->infect_species;
+        f.infect_from = h->infect_from;
+        f.dose = h->dose;
         for (int s = 0; s < h->n_species; ++s) {
             f.active[s] = r < h->substeps[s];
             f.last[s] = r == h->substeps[s] - 1;
@@ -453,6 +470,11 @@ int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
         for (int c = 0; c < h->g.ncol && rc == GLZ_OK; ++c) rc = sweep_pass(h, c);
         if (ms) CU(cudaEventRecord(ev[1], h->stream));
         if (rc == GLZ_OK && h->n_species > 0) rc = field_step(h);
+        if (rc == GLZ_OK && h->infect_species >= 0) {
+            const cudaError_t e = glz::launch_infection(h->cell_type, h->dose, (int)h->n_labels, h->infect_from,
+                                                        h->infect_to, h->infect_threshold, h->stream);
+            if (e != cudaSuccess) rc = fail(GLZ_DRIVER, std::string("infection: ") + cudaGetErrorString(e));
+        }
         if (ms) CU(cudaEventRecord(ev[2], h->stream));
         if (rc == GLZ_OK && h->has_pop) rc = population(h);
         if (ms) CU(cudaEventRecord(ev[3], h->stream));
@@ -752,8 +774,25 @@ int glz_gpu_cell_types(glz_gpu *h, uint8_t *out, size_t *count) {
         *count = h->n_labels;
         return fail(GLZ_INVALID, "the buffer is shorter than the label count");
     }
-    std::memcpy(out, h->cell_type_host.data(), h->n_labels);
+    CU(cudaMemcpyAsync(out, h->cell_type, h->n_labels, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
     *count = h->n_labels;
+    return GLZ_OK;
+}
+
+int glz_gpu_set_infection(glz_gpu *h, int species, int from_type, int to_type, double threshold) {
+    if (!h) return fail(GLZ_INVALID, "null handle");
+    if (species < 0 || species >= h->n_species) return fail(GLZ_INVALID, "the infection names no species of the model");
+    if (from_type < 1 || from_type >= h->n_types || to_type < 1 || to_type >= h->n_types || from_type == to_type)
+        return fail(GLZ_INVALID, "the infection switches between two distinct cell types (not the medium)");
+    if (!(threshold >= 0.0) || !(threshold * (double)glz::kDoseScale < 9.0e18))
+        return fail(GLZ_INVALID, "the infection threshold must be finite and >= 0");
+    h->infect_species = species;
+    h->infect_from = from_type;
+    h->infect_to = to_type;
+    h->infect_threshold = std::llround(threshold * (double)glz::kDoseScale);
+    // types now change during a run: the sweep reads them per copy
+    h->uniform = -1;
     return GLZ_OK;
 }
 
@@ -795,7 +834,7 @@ void glz_gpu_destroy(glz_gpu *h) {
     cudaFree(h->contact); cudaFree(h->tv); cudaFree(h->lv); cudaFree(h->ts); cudaFree(h->ls);
     cudaFree(h->chemo); cudaFree(h->sec); cudaFree(h->upt);
     cudaFree(h->tl); cudaFree(h->ll); cudaFree(h->divv); cudaFree(h->death); cudaFree(h->connected);
-    cudaFree(h->labels); cudaFree(h->cell_type); cudaFree(h->field_buf);
+    cudaFree(h->labels); cudaFree(h->cell_type); cudaFree(h->field_buf); cudaFree(h->dose);
     cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->counters);
     free_tallies(h->t);
     free_population(h);

@@ -137,9 +137,23 @@ struct FieldLaunch {
     const uint32_t *labels;
     const uint8_t *cell_type;
     const float *secretion, *uptake;
+    // the infection rule (an extension): the uptake of species infect_species
+    // by cells of type infect_from adds into dose[label], in units of 2^-24
+    int infect_species = -1;  // -1: no rule
+    int infect_from;
+    unsigned long long *dose;
 };
 
 cudaError_t launch_field_round(const FieldLaunch &a, cudaStream_t stream);
+
+// A cell of type `from` whose dose has reached `threshold` (units of 2^-24)
+// turns to type `to`.
+cudaError_t launch_infection(uint8_t *cell_type, const unsigned long long *dose, int n_labels, int from, int to,
+                             long long threshold, cudaStream_t stream);
+
+// Fixed-point scale of the infection dose: an uptake amount u adds
+// rint(u * 2^24), so the sum is exact and its order does not matter.
+constexpr float kDoseScale = 16777216.0f;
 
 // Recount every tally from the lattice into base slot `slot`, clearing every
 // delta word: volume, per-colour volume, surface, anchor (first site in scan

@@ -9,6 +9,10 @@
 // labels and every species once per Monte Carlo step:
 //   out = u + d (sum of faces - faces u) - decay u          (field.rs:110-130)
 //   on owned sites: v = out + sec; v -= upt v; v = max(v, 0) (field.rs:133-149)
+// With an infection rule set (glz_gpu_set_infection, an extension), the
+// uptake upt v of the rule's species by cells of the rule's type is summed
+// per cell in fixed point, and infection_kernel switches the cells whose sum
+// has reached the threshold.
 // Exchange reads only its own species, so running it right after that
 // species' last sub-step is the reference's order.
 
@@ -17,14 +21,43 @@
 
 namespace glz {
 
+// Add each lane's `amount` into dose[label] through the first lane of each
+// run of equal labels in the warp: one atomic per run. Every lane of the warp
+// takes part; a lane with nothing to add passes label kNoDose.
+constexpr uint32_t kNoDose = 0xffffffffu;
+
+__device__ __forceinline__ void add_dose(unsigned long long *dose, uint32_t label, long long amount) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint32_t before = __shfl_up_sync(full, label, 1);
+    const bool head = lane == 0 || label != before;
+    const unsigned heads = __ballot_sync(full, head);
+    long long scan = amount;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long v = __shfl_up_sync(full, scan, o);
+        if (lane >= o) scan += v;
+    }
+    const unsigned later = heads & ~(full >> (31 - lane));
+    const int last = later ? __ffs(later) - 2 : 31;
+    const long long scan_last = __shfl_sync(full, scan, last);
+    if (head && label != kNoDose) {
+        const long long run = scan_last - scan + amount;
+        if (run != 0) atomicAdd(&dose[label], (unsigned long long)run);
+    }
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(256) field_round_kernel(const __grid_constant__ FieldLaunch a) {
     const int W = a.g.w, H = a.g.h, D = a.g.d;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)a.g.sites) return;
-    const int x = (int)(i % W);
-    const int y = (int)((i / W) % H);
-    const int z = DIM == 3 ? (int)(i / ((size_t)W * H)) : 0;
+    const bool in = i < (size_t)a.g.sites;
+    // with an infection rule every lane stays for the warp's dose sums
+    if (!in && a.infect_species < 0) return;
+    const size_t c = in ? i : 0;
+    const int x = (int)(c % W);
+    const int y = (int)((c / W) % H);
+    const int z = DIM == 3 ? (int)(c / ((size_t)W * H)) : 0;
     const size_t row = ((size_t)z * H + y) * W;
     const size_t xm = row + (x == 0 ? W - 1 : x - 1);
     const size_t xp = row + (x == W - 1 ? 0 : x + 1);
@@ -37,33 +70,55 @@ __global__ void __launch_bounds__(256) field_round_kernel(const __grid_constant_
     }
     const float faces = DIM == 3 ? 6.0f : 4.0f;
     int type = -1;
+    uint32_t label = 0;
     for (int s = 0; s < a.n_species; ++s) {
         if (!a.active[s]) continue;
-        const float *__restrict__ u = a.in[s];
-        const float here = u[i];
-        float sum = u[xm];
-        sum = __fadd_rn(sum, u[xp]);
-        sum = __fadd_rn(sum, u[ym]);
-        sum = __fadd_rn(sum, u[yp]);
-        if (DIM == 3) {
-            sum = __fadd_rn(sum, u[zm]);
-            sum = __fadd_rn(sum, u[zp]);
-        }
-        float v = __fsub_rn(__fadd_rn(here, __fmul_rn(a.d[s], __fsub_rn(sum, __fmul_rn(faces, here)))),
-                            __fmul_rn(a.decay[s], here));
-        if (a.last[s]) {
-            if (type < 0) {
-                const uint32_t l = a.labels[i];
-                type = l == 0 ? 0x7fffffff : a.cell_type[l];
+        long long taken = 0;  // this site's uptake of the infection species, fixed point
+        if (in) {
+            const float *__restrict__ u = a.in[s];
+            const float here = u[i];
+            float sum = u[xm];
+            sum = __fadd_rn(sum, u[xp]);
+            sum = __fadd_rn(sum, u[ym]);
+            sum = __fadd_rn(sum, u[yp]);
+            if (DIM == 3) {
+                sum = __fadd_rn(sum, u[zm]);
+                sum = __fadd_rn(sum, u[zp]);
             }
-            if (type != 0x7fffffff) {
-                v = __fadd_rn(v, a.secretion[type * a.n_species + s]);
-                v = __fsub_rn(v, __fmul_rn(a.uptake[type * a.n_species + s], v));
-                v = v < 0.0f ? 0.0f : v;
+            float v = __fsub_rn(__fadd_rn(here, __fmul_rn(a.d[s], __fsub_rn(sum, __fmul_rn(faces, here)))),
+                                __fmul_rn(a.decay[s], here));
+            if (a.last[s]) {
+                if (type < 0) {
+                    label = a.labels[i];
+                    type = label == 0 ? 0x7fffffff : a.cell_type[label];
+                }
+                if (type != 0x7fffffff) {
+                    v = __fadd_rn(v, a.secretion[type * a.n_species + s]);
+                    const float amount = __fmul_rn(a.uptake[type * a.n_species + s], v);
+                    if (s == a.infect_species && type == a.infect_from)
+                        taken = __float2ll_rn(__fmul_rn(amount, kDoseScale));
+                    v = __fsub_rn(v, amount);
+                    v = v < 0.0f ? 0.0f : v;
+                }
             }
+            a.out[s][i] = v;
         }
-        a.out[s][i] = v;
+        if (s == a.infect_species && a.last[s])
+            add_dose(a.dose, in && type == a.infect_from ? label : kNoDose, taken);
     }
+}
+
+__global__ void infection_kernel(uint8_t *cell_type, const unsigned long long *dose, int n_labels, int from, int to,
+                                 long long threshold) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l == 0 || l >= n_labels) return;
+    if (cell_type[l] == from && (long long)dose[l] >= threshold) cell_type[l] = (uint8_t)to;
+}
+
+cudaError_t launch_infection(uint8_t *cell_type, const unsigned long long *dose, int n_labels, int from, int to,
+                             long long threshold, cudaStream_t stream) {
+    infection_kernel<<<(n_labels + 255) / 256, 256, 0, stream>>>(cell_type, dose, n_labels, from, to, threshold);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_field_round(const FieldLaunch &a, cudaStream_t stream) {

@@ -152,6 +152,12 @@ class GpuSimulation:
     def cell_types(self) -> np.ndarray:
         return self._per_label("glz_gpu_cell_types", np.uint8)
 
+    def set_infection(self, species: int, from_type: int, to_type: int, threshold: float) -> None:
+        """The infection rule (an extension; glazier has none): after each
+        step's field update, a cell of type `from_type` whose summed uptake
+        of field `species` has reached `threshold` turns to `to_type`."""
+        check(_lib.lib().glz_gpu_set_infection(self._h, int(species), int(from_type), int(to_type), float(threshold)))
+
     def set_nematic_field(self, pairs) -> None:
         flat = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1)
         check(_lib.lib().glz_gpu_set_nematic_field(self._h, ptr(flat), flat.size))

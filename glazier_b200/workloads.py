@@ -130,3 +130,68 @@ def adjoint_start(seed: int = 1, size: int = 512, side: int = 8) -> Start:
     for c in order[cells // 16: cells // 16 + 32]:
         start.cell_type[c] = 3
     return start
+
+
+# The infection rule of the two-field infection model, for set_infection:
+# (field, from type, to type, threshold) -- a healthy cell that has taken up
+# 5 units of virus is infected.
+INFECTION_RULE = (0, 1, 2, 5.0)
+
+
+def infection_start(seed: int = 1, size: int = 256, side: int = 8, grid: int = 16, immune: int = 32,
+                    immune_side: int = 6) -> Start:
+    """The two-field infection model on a periodic `size` lattice: a centred
+    `grid` x `grid` block of square cells of `side` (healthy, the centre one
+    infected), medium elsewhere, and `immune` squares of `immune_side` placed
+    uniformly at random in the medium (no overlap) by the hash of (seed,
+    attempt). Types: medium, healthy, infected, immune. Fields: virus (D 0.05,
+    decay 0.01) and interferon (D 0.1, decay 0.005). Infected cells secrete
+    virus at 1.0 and interferon at 0.5 per site per MCS and die at 0.005 per
+    MCS; healthy cells take up virus at 0.02; healthy and infected cells divide
+    at volume 128; immune cells climb interferon (chemotaxis 50) under a
+    length term (lambda_L 2, L_target 12). J is 10 between cells and 16
+    against the medium, every cell type keeps its cells in one piece, T 10.
+    The switch from healthy to infected is INFECTION_RULE, set on the engine
+    (or the replay) separately."""
+    vt = float(side * side)
+    epithelial = dict(target_volume=vt, lambda_volume=2.0, division_volume=2.0 * vt, connected=True)
+    n = 4
+    contact = [0.0 if (a == 0 and b == 0) else (16.0 if (a == 0 or b == 0) else 10.0)
+               for a in range(n) for b in range(n)]
+    model = Model(
+        width=size,
+        height=size,
+        contact=contact,
+        types=[CellType(), CellType(**epithelial), CellType(death_rate=0.005, **epithelial),
+               CellType(target_volume=float(immune_side * immune_side), lambda_volume=2.0, target_length=12.0,
+                        lambda_length=2.0, connected=True)],
+        temperature=10.0,
+        neighbour_order=2,
+        seed=seed,
+        species=[Species("virus", 0.05, 0.01, 0.0), Species("interferon", 0.1, 0.005, 0.0)],
+        secretion=[[0.0, 0.0], [0.0, 0.0], [1.0, 0.5], [0.0, 0.0]],
+        uptake=[[0.0, 0.0], [0.02, 0.0], [0.0, 0.0], [0.0, 0.0]],
+        chemotaxis=[[0.0, 0.0], [0.0, 0.0], [0.0, 0.0], [0.0, 50.0]],
+    )
+    model.validate()
+    labels = np.zeros((size, size), dtype=np.uint32)
+    origin = (size - grid * side) // 2
+    for gy in range(grid):
+        for gx in range(grid):
+            y0, x0 = origin + gy * side, origin + gx * side
+            labels[y0:y0 + side, x0:x0 + side] = 1 + gy * grid + gx
+    types = [1] * (grid * grid)
+    types[(grid // 2) * grid + grid // 2] = 2
+    placed, attempt = 0, 0
+    while placed < immune:
+        x0 = int(uniform01(seed, attempt, 11) * (size - immune_side + 1))
+        y0 = int(uniform01(seed, attempt, 12) * (size - immune_side + 1))
+        attempt += 1
+        if attempt > 100000:
+            raise ValueError("no room for the immune cells")
+        if labels[y0:y0 + immune_side, x0:x0 + immune_side].any():
+            continue
+        placed += 1
+        labels[y0:y0 + immune_side, x0:x0 + immune_side] = grid * grid + placed
+        types.append(3)
+    return Start(model, labels.reshape(-1), np.array([1] + types, dtype=np.uint8))

@@ -121,6 +121,16 @@ int glz_gpu_surfaces(glz_gpu *h, int64_t *out, size_t *count);
  * `*count` as for glz_gpu_volumes. */
 int glz_gpu_cell_types(glz_gpu *h, uint8_t *out, size_t *count);
 
+/* The infection rule of the two-field infection model, an extension with no
+ * reference counterpart (glazier's types only change by division): after
+ * each step's field update, a cell of type `from_type` whose summed uptake of
+ * species `species` has reached `threshold` turns to type `to_type`. The
+ * uptake is the exchange's upt * v per site (field.rs:133-149), summed per
+ * cell in fixed point (units of 2^-24, rounded to nearest per site), so the
+ * sum is exact and independent of order. Daughters start at zero. Set it
+ * before stepping; it stays for the handle's life. */
+int glz_gpu_set_infection(glz_gpu *h, int species, int from_type, int to_type, double threshold);
+
 /* Replace the nematic field, 2 * sites values: GpuSimulation::set_nematic_field
  * (lib.rs:1199-1221). A model without a nematic coupling is refused with the
  * reference's message. */

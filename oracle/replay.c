@@ -178,6 +178,11 @@ typedef struct {
     float *fields, *scratch;
     uint64_t mcs;
     uint64_t accepted;
+    /* the infection rule (glz_gpu_set_infection): species -1 is none; dose per
+     * label in units of 2^-24 */
+    int inf_species, inf_from, inf_to;
+    int64_t inf_threshold;
+    int64_t *dose;
 } rsim;
 
 static char rp_error[256];
@@ -193,6 +198,8 @@ static void reserve(rsim *s, size_t want) {
     s->volc = (int32_t *)realloc(s->volc, cap * s->ncol * sizeof(int32_t));
     s->anchor = (int32_t *)realloc(s->anchor, cap * 3 * sizeof(int32_t));
     s->mom = (int64_t *)realloc(s->mom, cap * s->nm * sizeof(int64_t));
+    s->dose = (int64_t *)realloc(s->dose, cap * sizeof(int64_t));
+    memset(s->dose + s->cap, 0, (cap - s->cap) * sizeof(int64_t));
     s->cap = cap;
 }
 
@@ -273,6 +280,7 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
         return NULL;
     }
     rsim *s = (rsim *)calloc(1, sizeof *s);
+    s->inf_species = -1;
     s->w = m->width;
     s->h = m->height;
     s->d = m->depth;
@@ -349,6 +357,7 @@ EXPORT void rp_destroy(rsim *s) {
     free(s->contact); free(s->tv); free(s->lv); free(s->ts); free(s->ls); free(s->tl); free(s->ll);
     free(s->div_vol); free(s->death); free(s->chemo); free(s->sec); free(s->upt); free(s->connected);
     free(s->fd); free(s->fdecay); free(s->substeps);
+    free(s->dose);
     free(s->labels); free(s->cell_type); free(s->vol); free(s->surf); free(s->volc); free(s->anchor);
     free(s->mom); free(s->fields); free(s->scratch);
     free(s);
@@ -611,7 +620,10 @@ static void field_step(rsim *s) {
                     if (l != 0) {
                         int t = s->cell_type[l];
                         v = v + s->sec[t * s->n_species + k];
-                        v = v - s->upt[t * s->n_species + k] * v;
+                        float amount = s->upt[t * s->n_species + k] * v;
+                        if (k == s->inf_species && t == s->inf_from)
+                            s->dose[l] += (int64_t)llrintf(amount * 16777216.0f);
+                        v = v - amount;
                         v = v < 0.0f ? 0.0f : v;
                     }
                 }
@@ -741,10 +753,25 @@ static void population(rsim *s) {
 
 /* One Monte Carlo step: the colour passes in order, the field step, then
  * division and death (lib.rs:1075-1141). */
+/* The infection rule, as glz_gpu_set_infection states it. */
+EXPORT int rp_set_infection(rsim *s, int species, int from_type, int to_type, double threshold) {
+    if (species < 0 || species >= s->n_species || from_type < 1 || from_type >= s->n_types || to_type < 1 ||
+        to_type >= s->n_types || from_type == to_type || !(threshold >= 0.0) || !(threshold * 16777216.0 < 9.0e18))
+        return 4;
+    s->inf_species = species;
+    s->inf_from = from_type;
+    s->inf_to = to_type;
+    s->inf_threshold = llround(threshold * 16777216.0);
+    return 0;
+}
+
 EXPORT void rp_step(rsim *s, uint64_t steps) {
     for (uint64_t r = 0; r < steps; ++r) {
         for (int c = 0; c < s->ncol; ++c) pass(s, c);
         if (s->n_species > 0) field_step(s);
+        if (s->inf_species >= 0)
+            for (size_t l = 1; l < s->n_labels; ++l)
+                if (s->cell_type[l] == s->inf_from && s->dose[l] >= s->inf_threshold) s->cell_type[l] = (uint8_t)s->inf_to;
         if (s->has_pop) population(s);
         s->mcs += 1;
     }

@@ -37,6 +37,8 @@ def lib():
                      "rp_moments", "rp_lengths"):
             getattr(L, name).argtypes = [P, P]
         L.rp_field.argtypes = [P, C.c_int, P]
+        L.rp_set_infection.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_double]
+        L.rp_set_infection.restype = C.c_int
         L.rp_expf.argtypes = [C.c_float]
         L.rp_expf.restype = C.c_float
         L.rp_draw.argtypes = [C.c_uint64, C.c_uint32, C.c_int32, C.c_int, C.c_int]
@@ -78,6 +80,11 @@ class ReplayOracle:
 
     def step(self, steps: int = 1) -> None:
         lib().rp_step(self.h, steps)
+
+    def set_infection(self, species: int, from_type: int, to_type: int, threshold: float) -> None:
+        """The infection rule of glz_gpu_set_infection, same arguments."""
+        if lib().rp_set_infection(self.h, species, from_type, to_type, float(threshold)):
+            raise ValueError("bad infection rule")
 
     @property
     def n_labels(self) -> int:

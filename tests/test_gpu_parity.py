@@ -171,3 +171,45 @@ def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, l
         for k in range(len(start.model.species)):
             assert np.array_equal(gpu.field(k).astype(np.float32), replay.field(k))
     gpu.close()
+
+
+@pytest.mark.parametrize("ctas", ["0", "3"])
+def test_the_infection_model_reproduces_the_replay_bit_for_bit(device, ctas, monkeypatch):
+    """The two-field infection model with its healthy-to-infected rule (an
+    extension with no reference counterpart, so its oracle is the replay with
+    the same rule): labels, volumes, surfaces, cell types and both fields
+    identical over 60 MCS, with infections taking place."""
+    from glazier_b200.workloads import INFECTION_RULE, infection_start
+
+    monkeypatch.setenv("GLAZIER_SWEEP_CTAS", ctas)
+    start = infection_start()
+    gpu = device.GpuSimulation.from_start(start)
+    replay = ReplayOracle.from_start(start)
+    gpu.set_infection(*INFECTION_RULE)
+    replay.set_infection(*INFECTION_RULE)
+    for chunk in (1, 29, 30):
+        gpu.step(chunk)
+        replay.step(chunk)
+        assert gpu.n_labels == replay.n_labels
+        labels = gpu.labels()
+        want = replay.labels()
+        assert np.array_equal(labels, want), f"{int((labels != want).sum())} sites differ after {gpu.mcs} MCS"
+        assert np.array_equal(gpu.volumes(), replay.volumes())
+        assert np.array_equal(gpu.surfaces(), replay.surfaces())
+        assert np.array_equal(gpu.cell_types(), replay.cell_types())
+        for k in range(2):
+            assert np.array_equal(gpu.field(k).astype(np.float32), replay.field(k))
+    types, vols = gpu.cell_types(), gpu.volumes()
+    assert int(((types == 2) & (vols > 0)).sum()) > 3
+    gpu.close()
+
+
+def test_a_bad_infection_rule_is_refused(device):
+    from glazier_b200.engine import GpuError
+    from glazier_b200.workloads import infection_start
+
+    gpu = device.GpuSimulation.from_start(infection_start())
+    for rule in ((2, 1, 2, 5.0), (0, 0, 2, 5.0), (0, 1, 1, 5.0), (0, 1, 2, -1.0), (0, 1, 2, 1e12)):
+        with pytest.raises(GpuError):
+            gpu.set_infection(*rule)
+    gpu.close()

@@ -148,3 +148,37 @@ def test_the_replay_field_matches_the_f64_field_step():
     assert np.array_equal(r.labels(), cpu.labels())
     f32, f64 = r.field(0).astype(np.float64), cpu.field(0)
     assert np.max(np.abs(f32 - f64) / np.maximum(np.abs(f64), 1e-30)) < 1e-5
+
+
+def test_the_infection_rule_spreads_and_only_from_healthy_cells():
+    """The infection rule (an extension, no reference counterpart): over 40
+    MCS of the two-field infection model the centre cell's virus infects its
+    neighbours; without the rule the healthy cells stay healthy; a threshold
+    no cell can reach switches none; a bad rule is refused."""
+    from glazier_b200.workloads import INFECTION_RULE, infection_start
+
+    def run(rule, steps=40):
+        st = infection_start()
+        r = R.ReplayOracle.from_start(st)
+        if rule is not None:
+            r.set_infection(*rule)
+        r.step(steps)
+        return st, r.cell_types(), r.volumes()
+
+    st, types, vols = run(INFECTION_RULE)
+    alive = vols > 0
+    infected = int(((types == 2) & alive).sum())
+    assert infected > 3
+    # immune cells (type 3) never switch
+    assert np.array_equal(types[257:289], st.cell_type[257:289])
+    _, plain, _ = run(None)
+    assert int((plain[1:257] == 2).sum()) == 1
+    _, high, _ = run((0, 1, 2, 1e9))
+    assert np.array_equal(high[:257], plain[:257])
+    r = R.ReplayOracle.from_start(infection_start())
+    with pytest.raises(ValueError):
+        r.set_infection(0, 1, 1, 5.0)
+    with pytest.raises(ValueError):
+        r.set_infection(2, 1, 2, 5.0)
+    with pytest.raises(ValueError):
+        r.set_infection(0, 1, 2, 1e12)  # past the fixed-point range
