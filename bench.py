@@ -240,6 +240,40 @@ def adjoint_compare(steps: int, every: int, repeats: int, device: int) -> dict:
             "note": "fields are 1 MB each: the working set sits in L2, so HBM is not the bound here"}
 
 
+def infection_compare(mcs: int, cpu_mcs: int, device: int) -> dict:
+    """The two-field infection model at 256^2 (centred 16 x 16 tissue with one
+    infected cell, 32 immune cells at random in the medium; fields, division,
+    death, length, chemotaxis and the connectivity veto all on) with its
+    infection rule: `mcs` MCS on the device from the start, phases timed with
+    CUDA events. Beside it the serial engine (the pinned restatement of the
+    reference's CPU engine, one core) on the same start without the rule, which
+    the reference does not have, over `cpu_mcs` MCS."""
+    from glazier_b200.engine import GpuSimulation
+    from glazier_b200.workloads import INFECTION_RULE, infection_start
+    from oracle.serial import SerialOracle
+
+    start = infection_start()
+    sites = start.model.sites
+    sim = GpuSimulation.from_start(start, device=device)
+    sim.set_infection(*INFECTION_RULE)
+    ms = sim.step_profiled(mcs)
+    types, vols = sim.cell_types(), sim.volumes()
+    infected = int(((types == 2) & (vols > 0)).sum())
+    cells = int((vols[1:] > 0).sum())
+    sim.close()
+    total = sum(ms)
+    o = SerialOracle.from_start(start)
+    t = time.perf_counter()
+    o.step(cpu_mcs)
+    cpu_s = time.perf_counter() - t
+    return {"lattice": "256x256", "mcs": mcs, "device_ms": total,
+            "phase_ms": {"sweep": ms[0], "fields": ms[1], "population": ms[2]},
+            "site_updates_per_s": sites * mcs / (total / 1e3), "live_cells_end": cells,
+            "infected_end": infected,
+            "cpu_serial": {"mcs": cpu_mcs, "seconds": cpu_s, "site_updates_per_s": sites * cpu_mcs / cpu_s,
+                           "cores": 1, "kind": "port", "note": "same start, infection rule off (the reference has none)"}}
+
+
 def cpu_baseline(size: int, seconds: float) -> dict:
     """The serial engine on one host core, a bounded sample of the same lattice."""
     from oracle.serial import SerialOracle
@@ -413,6 +447,8 @@ def run_ours(args) -> None:
     }
     if world == 1 and not args.no_ensemble:
         line["ensemble"] = ensemble_compare(100, torch.cuda.current_device())
+    if world == 1 and not args.no_infection:
+        line["infection"] = infection_compare(200, 20, torch.cuda.current_device())
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_compare(50, 10, 5, torch.cuda.current_device())
     if world == 1 and not args.no_cpu_baseline:
@@ -432,6 +468,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-infection", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

@@ -232,6 +232,19 @@ class Blueprint:
     def nematic_field(self):
         return self.raw.get("nematic_field")
 
+    def infection_rule(self):
+        """The optional `infection` object, an extension glazier's reader does
+        not have: ``{"field": name, "from": type, "to": type, "threshold": x}``
+        as (field index, from type, to type, threshold) in the engine's
+        indices (type 0 the medium), or None."""
+        spec = self.raw.get("infection")
+        if spec is None:
+            return None
+        fields = [f["name"] for f in self.fields]
+        names = [t["name"] for t in self.types]
+        return (fields.index(spec["field"]), names.index(spec["from"]) + 1, names.index(spec["to"]) + 1,
+                float(spec["threshold"]))
+
     @classmethod
     def from_json(cls, text: str) -> "Blueprint":
         """blueprint.rs:385-447: parse, fill serde defaults, cross-check."""
@@ -295,6 +308,19 @@ class Blueprint:
                         raise BlueprintError(
                             f"type {spec['name']} states {what} of {name}, which is not a field this description declares"
                         )
+        infection = raw.get("infection")
+        if infection is not None:
+            _require(infection, ("field", "from", "to", "threshold"), "the infection rule")
+            if infection["field"] not in known:
+                raise BlueprintError(f"the infection rule names the field {infection['field']}, which the description does not declare")
+            for key in ("from", "to"):
+                if infection[key] not in names:
+                    raise BlueprintError(f"the infection rule names the type {infection[key]}, which the description does not state")
+            if infection["from"] == infection["to"]:
+                raise BlueprintError("the infection rule switches a type to itself")
+            threshold = infection["threshold"]
+            if not isinstance(threshold, (int, float)) or not threshold >= 0:
+                raise BlueprintError("the infection threshold must be a number >= 0")
         bp.model().validate()
         return bp
 

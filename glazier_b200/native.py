@@ -35,6 +35,8 @@ def _simulate(text: str, steps, base: str = "."):
     except BlueprintError as e:
         raise ValueError(str(e)) from None
     sim = GpuSimulation.from_start(start)
+    if bp.infection_rule() is not None:
+        sim.set_infection(*bp.infection_rule())
     sim.step(bp.steps if steps is None else int(steps))
     return bp, sim
 
@@ -66,6 +68,8 @@ class GpuSession:
         except BlueprintError as e:
             raise ValueError(str(e)) from None
         self._sim = GpuSimulation.from_start(start)
+        if bp.infection_rule() is not None:
+            self._sim.set_infection(*bp.infection_rule())
         self._sites = bp.width * bp.height * bp.depth
 
     def step(self, steps: int) -> None:

@@ -113,6 +113,35 @@ def test_the_reader_refuses_what_the_reference_refuses():
         Blueprint.from_json(json.dumps(bad))
 
 
+def test_the_reader_takes_an_infection_rule_and_refuses_a_bad_one():
+    """The `infection` key is an extension glazier's reader lacks: a good rule
+    comes back in engine indices (field, from type, to type, threshold), a
+    rule naming something undeclared is refused."""
+    import copy
+    import json
+
+    base = {
+        "name": "x", "width": 16, "height": 16,
+        "types": [{"name": "Healthy", "target_volume": 16, "lambda_volume": 1, "uptake": {"virus": 0.02}},
+                  {"name": "Infected", "target_volume": 16, "lambda_volume": 1, "secretion": {"virus": 1.0}}],
+        "fields": [{"name": "virus", "diffusion": 0.05}],
+        "contact": [0, 16, 16, 16, 10, 10, 16, 10, 10], "temperature": 10, "neighbour_order": 2, "seed": 1,
+        "steps": 1, "dump_every": 0, "initial": {"side": 4, "nx": 2, "ny": 2},
+        "units": {"micron_per_site": 1, "minute_per_step": 1},
+        "infection": {"field": "virus", "from": "Healthy", "to": "Infected", "threshold": 5},
+    }
+    assert Blueprint.from_json(json.dumps(base)).infection_rule() == (0, 1, 2, 5.0)
+    plain = copy.deepcopy(base)
+    del plain["infection"]
+    assert Blueprint.from_json(json.dumps(plain)).infection_rule() is None
+    for key, value, message in (("field", "toxin", "does not declare"), ("to", "Immune", "does not state"),
+                                ("to", "Healthy", "to itself"), ("threshold", -1, ">= 0")):
+        bad = copy.deepcopy(base)
+        bad["infection"][key] = value
+        with pytest.raises(BlueprintError, match=message):
+            Blueprint.from_json(json.dumps(bad))
+
+
 def test_initial_types_hand_out_rounded_shares_in_order():
     # blueprint.rs:247-261: 2% of 256 is 5.12, so five cells, the first five
     import json

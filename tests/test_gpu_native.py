@@ -68,3 +68,33 @@ def test_every_reference_blueprint_the_engine_runs_starts_and_steps(device):
         session.step(2)
         ran += 1
     assert ran >= 8
+
+
+def test_a_session_applies_the_descriptions_infection_rule(device):
+    """A description with the `infection` extension key: the session's engine
+    switches healthy cells to infected as their virus uptake passes the
+    threshold; the same description without the key switches none."""
+    text = {
+        "name": "infection rule", "width": 64, "height": 64,
+        "types": [{"name": "Healthy", "target_volume": 64, "lambda_volume": 2, "uptake": {"virus": 0.05}},
+                  {"name": "Infected", "target_volume": 64, "lambda_volume": 2, "secretion": {"virus": 2.0}}],
+        "fields": [{"name": "virus", "diffusion": 0.2, "decay": 0.01}],
+        "contact": [0, 16, 16, 16, 10, 10, 16, 10, 10], "temperature": 10, "neighbour_order": 2, "seed": 3,
+        "steps": 30, "dump_every": 0, "initial": {"side": 8, "nx": 8, "ny": 8, "fractions": {"Infected": 0.05}},
+        "units": {"micron_per_site": 1, "minute_per_step": 1},
+        "infection": {"field": "virus", "from": "Healthy", "to": "Infected", "threshold": 3},
+    }
+    counts = []
+    for with_rule in (True, False):
+        spec = dict(text)
+        if not with_rule:
+            del spec["infection"]
+        session = native.GpuSession(json.dumps(spec))
+        before = int((session.simulation.cell_types()[1:] == 2).sum())
+        session.step(30)
+        counts.append((before, int((session.simulation.cell_types()[1:] == 2).sum())))
+        session.simulation.close()
+    (before, after), (plain_before, plain_after) = counts
+    assert before == plain_before > 0
+    assert after > before
+    assert plain_after == plain_before
