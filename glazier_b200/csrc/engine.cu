@@ -109,13 +109,13 @@ struct glz_gpu {
     int n_types = 0, n_species = 0;
     float beta = 0.0f;
     uint64_t seed = 0;
-    bool has_length = false, tracks = false, has_chemotaxis = false, has_pop = false;
+    bool has_length = false, tracks = false, has_chemotaxis = false, has_pop = false, has_external = false;
     int substeps[glz::kMaxSpecies] = {};
     float fd[glz::kMaxSpecies] = {}, fdecay[glz::kMaxSpecies] = {};
 
     // per-type tables
     float *contact = nullptr, *tv = nullptr, *lv = nullptr, *ts = nullptr, *ls = nullptr;
-    float *chemo = nullptr, *sec = nullptr, *upt = nullptr;
+    float *chemo = nullptr, *sec = nullptr, *upt = nullptr, *ext = nullptr;
     double *tl = nullptr, *ll = nullptr, *divv = nullptr, *death = nullptr;
     uint8_t *connected = nullptr;
 
@@ -165,6 +165,7 @@ struct glz_gpu {
         tt.death_rate = death;
         tt.connected = connected;
         tt.chemotaxis = chemo;
+        tt.external = ext;
         tt.secretion = sec;
         tt.uptake = upt;
         return tt;
@@ -360,6 +361,7 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.has_length = h->has_length;
     a.tracks = h->tracks;
     a.has_chemotaxis = h->has_chemotaxis;
+    a.has_external = h->has_external;
     for (int s = 0; s < h->n_species; ++s) a.fields[s] = h->field_ptr(s, h->field_cur[s]);
     a.use_tma = h->use_tma;
     a.lean = h->lean;
@@ -533,7 +535,6 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     }
     if (nematic) return fail(GLZ_UNSUPPORTED, "the device engine does not run the nematic term");
     if (motility) return fail(GLZ_UNSUPPORTED, "the device engine does not run the motility (Act) term");
-    if (drift) return fail(GLZ_UNSUPPORTED, "the device engine does not run the external drift term");
     if (activity)
         for (long long i = 0; i < sites; ++i)
             if (activity[i] != 0.0) return fail(GLZ_UNSUPPORTED, "a nonzero activity needs the motility term");
@@ -587,6 +588,9 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         h->has_pop |= divv[k] > 0.0 || death[k] > 0.0;
     }
     h->tracks = h->has_length || h->has_pop;
+    std::vector<float> ext(3 * (size_t)nt);
+    for (size_t i = 0; i < ext.size(); ++i) ext[i] = (float)at(m->external, i);
+    h->has_external = drift;
     std::vector<float> chemo(nt * (size_t)ns), sec(nt * (size_t)ns), upt(nt * (size_t)ns);
     for (size_t i = 0; i < chemo.size(); ++i) {
         chemo[i] = (float)at(m->chemotaxis, i);
@@ -616,7 +620,8 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
 
     // GLAZIER_SWEEP_LEAN=0 keeps every model on the general sweep kernel.
     const char *lean_env = std::getenv("GLAZIER_SWEEP_LEAN");
-    h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !has_conn && !(lean_env && lean_env[0] == '0');
+    h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !h->has_external && !has_conn &&
+              !(lean_env && lean_env[0] == '0');
     h->host_tv = tv;
     h->host_lv = lv;
     h->host_ts = ts;
@@ -626,7 +631,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         (rc = upload(h, &h->ts, ts)) || (rc = upload(h, &h->ls, ls)) || (rc = upload(h, &h->tl, tl)) ||
         (rc = upload(h, &h->ll, ll)) || (rc = upload(h, &h->divv, divv)) || (rc = upload(h, &h->death, death)) ||
         (rc = upload(h, &h->connected, conn)) || (rc = upload(h, &h->chemo, chemo)) || (rc = upload(h, &h->sec, sec)) ||
-        (rc = upload(h, &h->upt, upt)))
+        (rc = upload(h, &h->upt, upt)) || (rc = upload(h, &h->ext, ext)))
         return bail(rc);
 
     if ((rc = dev_alloc(&h->labels, (size_t)sites))) return bail(rc);
@@ -832,7 +837,7 @@ void glz_gpu_destroy(glz_gpu *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->contact); cudaFree(h->tv); cudaFree(h->lv); cudaFree(h->ts); cudaFree(h->ls);
-    cudaFree(h->chemo); cudaFree(h->sec); cudaFree(h->upt);
+    cudaFree(h->chemo); cudaFree(h->sec); cudaFree(h->upt); cudaFree(h->ext);
     cudaFree(h->tl); cudaFree(h->ll); cudaFree(h->divv); cudaFree(h->death); cudaFree(h->connected);
     cudaFree(h->labels); cudaFree(h->cell_type); cudaFree(h->field_buf); cudaFree(h->dose);
     cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->counters);

@@ -31,6 +31,7 @@ struct TypeTables {
     const double *target_length, *lambda_length, *division_volume, *death_rate;
     const uint8_t *connected;
     const float *chemotaxis, *secretion, *uptake;  // n_types * n_species
+    const float *external;                         // n_types * 3: the drift vector
 };
 
 // The per-cell tallies a colour pass reads, in the rotation that gives every
@@ -77,7 +78,7 @@ struct SweepLaunch {
     int uniform_contact_exact;  // J m is exact in f32 for every |m| <= n_off (see sweep.cu)
     float uniform_contact;      // J[type][type] when uniform
     float u_target_volume, u_lambda_volume, u_target_surface, u_lambda_surface;
-    int has_length, tracks, has_chemotaxis;
+    int has_length, tracks, has_chemotaxis, has_external;
     const float *fields[kMaxSpecies];
     int use_tma;
     int lean;                // take the lean kernel: no length, chemotaxis, connectivity or moment tracking

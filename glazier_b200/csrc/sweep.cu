@@ -243,14 +243,24 @@ __device__ __noinline__ float extra_terms(const SweepLaunch &a, uint32_t old, ui
             delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_new, nw, vol_new, terms, 1));
         }
     }
+    const int ox = a.g.off[pick][0], oy = a.g.off[pick][1], oz = a.g.off[pick][2];
+    const int sx = wrap(x + ox, W), sy = wrap(y + oy, H), sz = wrap(z + oz, D);
     if (a.has_chemotaxis && nw != 0) {
-        const int ox = a.g.off[pick][0], oy = a.g.off[pick][1], oz = a.g.off[pick][2];
-        const uint32_t source = (uint32_t)(((size_t)wrap(z + oz, D) * H + wrap(y + oy, H)) * W + wrap(x + ox, W));
+        const uint32_t source = (uint32_t)(((size_t)sz * H + sy) * W + sx);
         for (int s = 0; s < a.n_species; ++s) {
             const float lam = a.t.chemotaxis[t_new * a.n_species + s];
             if (lam == 0.0f) continue;
             const float *f = a.fields[s];
             delta = __fsub_rn(delta, __fmul_rn(lam, __fsub_rn(f[target], f[source])));
+        }
+    }
+    // The drift (cpu.rs:360-369, lib.rs:664-673): work e . (target - source),
+    // the step folded onto the lattice.
+    if (a.has_external && nw != 0) {
+        const float ex = a.t.external[3 * t_new], ey = a.t.external[3 * t_new + 1], ez = a.t.external[3 * t_new + 2];
+        if (ex != 0.0f || ey != 0.0f || ez != 0.0f) {
+            const float fx = (float)fold_int(x - sx, W), fy = (float)fold_int(y - sy, H), fz = (float)fold_int(z - sz, D);
+            delta = __fsub_rn(delta, __fadd_rn(__fadd_rn(__fmul_rn(ex, fx), __fmul_rn(ey, fy)), __fmul_rn(ez, fz)));
         }
     }
     return delta;
@@ -398,7 +408,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const int
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
         }
     }
-    if (EXTRAS && (a.has_length || a.has_chemotaxis))
+    if (EXTRAS && (a.has_length || a.has_chemotaxis || a.has_external))
         delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
 
     // Metropolis: a copy that lowers the energy (or keeps it) is taken, else

@@ -163,6 +163,8 @@ typedef struct {
     float beta; /* (float)(1 / T), rounded once on the host */
     uint64_t seed;
     float *contact, *tv, *lv, *ts, *ls, *chemo, *sec, *upt;
+    float *ext; /* 3 per type: the drift vector */
+    int has_external;
     double *tl, *ll, *div_vol, *death;
     uint8_t *connected;
     float *fd, *fdecay; /* per species per sub-step */
@@ -304,6 +306,8 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
     s->div_vol = f64_copy(m->division_volume, nt);
     s->death = f64_copy(m->death_rate, nt);
     s->chemo = f32_copy(m->chemotaxis, (size_t)nt * ns);
+    s->ext = f32_copy(m->external, 3 * (size_t)nt);
+    for (int i = 0; i < 3 * nt; ++i) s->has_external |= s->ext[i] != 0.0f;
     s->sec = f32_copy(m->secretion, (size_t)nt * ns);
     s->upt = f32_copy(m->uptake, (size_t)nt * ns);
     s->connected = (uint8_t *)calloc(nt, 1);
@@ -355,7 +359,7 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
 EXPORT void rp_destroy(rsim *s) {
     if (!s) return;
     free(s->contact); free(s->tv); free(s->lv); free(s->ts); free(s->ls); free(s->tl); free(s->ll);
-    free(s->div_vol); free(s->death); free(s->chemo); free(s->sec); free(s->upt); free(s->connected);
+    free(s->div_vol); free(s->death); free(s->chemo); free(s->sec); free(s->upt); free(s->ext); free(s->connected);
     free(s->fd); free(s->fdecay); free(s->substeps);
     free(s->dose);
     free(s->labels); free(s->cell_type); free(s->vol); free(s->surf); free(s->volc); free(s->anchor);
@@ -555,6 +559,15 @@ static void pass(rsim *s, int colour) {
                         if (lam == 0.0f) continue;
                         const float *f = &s->fields[(size_t)k * s->sites];
                         delta = delta - lam * (f[target] - f[source]);
+                    }
+                }
+                /* the drift, cpu.rs:360-369: work e . (target - source), folded */
+                if (nw != 0 && s->has_external) {
+                    float ex = s->ext[3 * t_new], ey = s->ext[3 * t_new + 1], ez = s->ext[3 * t_new + 2];
+                    if (ex != 0.0f || ey != 0.0f || ez != 0.0f) {
+                        float fx = (float)fold_int(x - sx, s->w), fy = (float)fold_int(y - sy, s->h),
+                              fz = (float)fold_int(z - sz, s->d);
+                        delta = delta - (ex * fx + ey * fy + ez * fz);
                     }
                 }
 

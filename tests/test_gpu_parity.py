@@ -105,6 +105,12 @@ def _connected():
     return tiled(m), 20
 
 
+def _drift():
+    # a drift along +x for the cells, diagonal pulls included (Moore picks)
+    m = sheet_model(seed=13, external=(0.75, -0.25, 0.0))
+    return tiled(m, 8, 6, 6), 25
+
+
 def _population():
     m = sheet_model(seed=8, division_volume=72.0, death_rate=0.005, target_volume=100.0)
     return tiled(m, 6, 6, 6), 40
@@ -139,6 +145,7 @@ CASES = {
     "length-volume": _length_volume,
     "connected": _connected,
     "population": _population,
+    "drift": _drift,
     "chemotaxis-ramp": _chemotaxis_ramp,
 }
 

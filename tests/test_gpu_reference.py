@@ -216,3 +216,40 @@ def test_the_device_and_the_serial_engine_agree_on_a_constrained_sheet(device):
     assert int(dv[1:].sum()) == int(cpu.volumes()[1:].sum())
     sc, sg = spread(cpu.volumes()[1:], 64.0), spread(dv[1:], 64.0)
     assert abs(sc - sg) / max(sc, sg) < 0.3, (sc, sg)
+
+
+def _lone_cell(model):
+    """motility.rs:35-45: one 8 x 8 cell at x, y in [44, 52) on an empty 96 x 96
+    lattice."""
+    labels = np.zeros((model.height, model.width), dtype=np.uint32)
+    labels[44:52, 44:52] = 1
+    return Start(model, labels.reshape(-1), np.array([1, 1], dtype=np.uint8))
+
+
+def _motility_model(max_activity, lambda_activity, external, connected):
+    # motility.rs:10-32
+    from glazier_b200.blueprint import CellType, Model
+
+    return Model(width=96, height=96, contact=[0.0, 16.0, 16.0, 8.0],
+                 types=[CellType(), CellType(target_volume=64.0, lambda_volume=2.0, connected=connected,
+                                             max_activity=max_activity, lambda_activity=lambda_activity,
+                                             external=tuple(external))],
+                 temperature=10.0, neighbour_order=2, seed=29)
+
+
+def _centroid(labels, width):
+    ys, xs = np.divmod(np.flatnonzero(np.asarray(labels) == 1), width)
+    return xs.mean(), ys.mean()
+
+
+@pytest.mark.parametrize("sign", [1.0, -1.0])
+def test_the_device_drifts_a_cell_the_way_it_points(device, sign):
+    # motility.rs:199-215 (device) and 107-132 (the reversed drift)
+    st = _lone_cell(_motility_model(0.0, 0.0, (3.0 * sign, 0.0, 0.0), True))
+    x0, y0 = _centroid(st.labels, 96)
+    gpu = device.GpuSimulation.from_start(st)
+    gpu.step(300)
+    x1, y1 = _centroid(gpu.labels(), 96)
+    gpu.close()
+    assert sign * (x1 - x0) > 5.0, f"the cell moved {x1 - x0} along x"
+    assert abs(y1 - y0) < 4.0, f"the cell wandered {y1 - y0} across the drift"
