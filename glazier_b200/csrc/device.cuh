@@ -66,6 +66,38 @@ __device__ __forceinline__ float metropolis_exp(float x) {
     return __fmul_rn(p, __int_as_float((ki + 127) << 23));
 }
 
+// Natural log for the motility term's geometric means, written from the
+// series ln m = 2 atanh(s) = 2 (s + s^3/3 + s^5/5 + s^7/7 + s^9/9 + ...),
+// s = (m - 1) / (m + 1) (Abramowitz and Stegun 4.1.27), on a mantissa m
+// reduced to [sqrt(1/2), sqrt(2)] so |s| < 0.172 and the terms past s^9 fall
+// below f32 precision; the exponent adds e ln 2 with ln 2 split hi + lo. Only
+// correctly rounded operations, so a host replay gets the same bits. For
+// x > 0 and finite.
+__device__ __forceinline__ float motility_log(float x) {
+    int e = 0;
+    if (x < 1.17549435e-38f) {  // subnormal: scale into the normal range
+        x = __fmul_rn(x, 16777216.0f);
+        e = -24;
+    }
+    const int bits = __float_as_int(x);
+    e += ((bits >> 23) & 0xff) - 127;
+    float m = __int_as_float((bits & 0x007fffff) | 0x3f800000);  // [1, 2)
+    if (m > 1.41421356f) {
+        m = __fmul_rn(m, 0.5f);
+        e += 1;
+    }
+    const float s = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+    const float s2 = __fmul_rn(s, s);
+    float p = 0.111111111f;
+    p = __fmaf_rn(p, s2, 0.142857143f);
+    p = __fmaf_rn(p, s2, 0.2f);
+    p = __fmaf_rn(p, s2, 0.333333333f);
+    p = __fmul_rn(p, s2);
+    const float lm = __fmul_rn(__fmul_rn(2.0f, s), __fadd_rn(1.0f, p));
+    const float fe = (float)e;
+    return __fadd_rn(__fmaf_rn(fe, 0.693145751953125f, lm), __fmul_rn(fe, 1.428606765330187e-06f));
+}
+
 __host__ __device__ __forceinline__ int wrap(int v, int n) {
     int r = v % n;
     return r < 0 ? r + n : r;

@@ -110,12 +110,16 @@ struct glz_gpu {
     float beta = 0.0f;
     uint64_t seed = 0;
     bool has_length = false, tracks = false, has_chemotaxis = false, has_pop = false, has_external = false;
+    bool has_motility = false;
+    float *activity = nullptr;  // sites, with motility
+    uint2 *pending = nullptr;   // a motility pass's accepted copies
+    int *pending_count = nullptr;
     int substeps[glz::kMaxSpecies] = {};
     float fd[glz::kMaxSpecies] = {}, fdecay[glz::kMaxSpecies] = {};
 
     // per-type tables
     float *contact = nullptr, *tv = nullptr, *lv = nullptr, *ts = nullptr, *ls = nullptr;
-    float *chemo = nullptr, *sec = nullptr, *upt = nullptr, *ext = nullptr;
+    float *chemo = nullptr, *sec = nullptr, *upt = nullptr, *ext = nullptr, *maxact = nullptr, *lamact = nullptr;
     double *tl = nullptr, *ll = nullptr, *divv = nullptr, *death = nullptr;
     uint8_t *connected = nullptr;
 
@@ -166,6 +170,8 @@ struct glz_gpu {
         tt.connected = connected;
         tt.chemotaxis = chemo;
         tt.external = ext;
+        tt.max_activity = maxact;
+        tt.lambda_activity = lamact;
         tt.secretion = sec;
         tt.uptake = upt;
         return tt;
@@ -362,6 +368,10 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.tracks = h->tracks;
     a.has_chemotaxis = h->has_chemotaxis;
     a.has_external = h->has_external;
+    a.has_motility = h->has_motility;
+    a.activity = h->activity;
+    a.pending = h->pending;
+    a.pending_count = h->pending_count;
     for (int s = 0; s < h->n_species; ++s) a.fields[s] = h->field_ptr(s, h->field_cur[s]);
     a.use_tma = h->use_tma;
     a.lean = h->lean;
@@ -369,6 +379,7 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.tensor_map = h->use_tma ? &h->tmap : nullptr;
     a.error_flag = h->error_flag;
     CU(glz::launch_sweep(a, h->stream));
+    if (h->has_motility) CU(glz::launch_apply_copies(a, h->activity, h->stream));
     h->pass_no += 1;
     return GLZ_OK;
 }
@@ -470,6 +481,10 @@ int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
     for (uint64_t r = 0; r < steps && rc == GLZ_OK; ++r) {
         if (ms) CU(cudaEventRecord(ev[0], h->stream));
         for (int c = 0; c < h->g.ncol && rc == GLZ_OK; ++c) rc = sweep_pass(h, c);
+        if (rc == GLZ_OK && h->has_motility) {
+            const cudaError_t e = glz::launch_activity_decay(h->activity, h->g.sites, h->stream);
+            if (e != cudaSuccess) rc = fail(GLZ_DRIVER, std::string("activity decay: ") + cudaGetErrorString(e));
+        }
         if (ms) CU(cudaEventRecord(ev[1], h->stream));
         if (rc == GLZ_OK && h->n_species > 0) rc = field_step(h);
         if (rc == GLZ_OK && h->infect_species >= 0) {
@@ -534,8 +549,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         for (int a = 0; a < 3; ++a) drift |= at(m->external, 3 * (size_t)k + a) != 0.0;
     }
     if (nematic) return fail(GLZ_UNSUPPORTED, "the device engine does not run the nematic term");
-    if (motility) return fail(GLZ_UNSUPPORTED, "the device engine does not run the motility (Act) term");
-    if (activity)
+    if (activity && !motility)
         for (long long i = 0; i < sites; ++i)
             if (activity[i] != 0.0) return fail(GLZ_UNSUPPORTED, "a nonzero activity needs the motility term");
     for (long long i = 0; i < sites; ++i)
@@ -588,6 +602,12 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         h->has_pop |= divv[k] > 0.0 || death[k] > 0.0;
     }
     h->tracks = h->has_length || h->has_pop;
+    std::vector<float> maxact(nt), lamact(nt);
+    for (int k = 0; k < nt; ++k) {
+        maxact[k] = (float)at(m->max_activity, k);
+        lamact[k] = (float)at(m->lambda_activity, k);
+    }
+    h->has_motility = motility;
     std::vector<float> ext(3 * (size_t)nt);
     for (size_t i = 0; i < ext.size(); ++i) ext[i] = (float)at(m->external, i);
     h->has_external = drift;
@@ -620,7 +640,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
 
     // GLAZIER_SWEEP_LEAN=0 keeps every model on the general sweep kernel.
     const char *lean_env = std::getenv("GLAZIER_SWEEP_LEAN");
-    h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !h->has_external && !has_conn &&
+    h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !h->has_external && !h->has_motility && !has_conn &&
               !(lean_env && lean_env[0] == '0');
     h->host_tv = tv;
     h->host_lv = lv;
@@ -631,7 +651,8 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         (rc = upload(h, &h->ts, ts)) || (rc = upload(h, &h->ls, ls)) || (rc = upload(h, &h->tl, tl)) ||
         (rc = upload(h, &h->ll, ll)) || (rc = upload(h, &h->divv, divv)) || (rc = upload(h, &h->death, death)) ||
         (rc = upload(h, &h->connected, conn)) || (rc = upload(h, &h->chemo, chemo)) || (rc = upload(h, &h->sec, sec)) ||
-        (rc = upload(h, &h->upt, upt)) || (rc = upload(h, &h->ext, ext)))
+        (rc = upload(h, &h->upt, upt)) || (rc = upload(h, &h->ext, ext)) || (rc = upload(h, &h->maxact, maxact)) ||
+        (rc = upload(h, &h->lamact, lamact)))
         return bail(rc);
 
     if ((rc = dev_alloc(&h->labels, (size_t)sites))) return bail(rc);
@@ -650,6 +671,16 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
             if (cudaMemcpy(h->field_ptr(s, 0), f.data(), sites * sizeof(float), cudaMemcpyHostToDevice))
                 return bail(fail(GLZ_DRIVER, "field upload failed"));
         }
+    }
+    if (h->has_motility) {
+        std::vector<float> act((size_t)sites);
+        for (long long i = 0; i < sites; ++i) act[i] = activity ? (float)activity[i] : 0.0f;
+        if ((rc = dev_alloc(&h->activity, (size_t)sites))) return bail(rc);
+        if (cudaMemcpy(h->activity, act.data(), sites * sizeof(float), cudaMemcpyHostToDevice))
+            return bail(fail(GLZ_DRIVER, "activity upload failed"));
+        if ((rc = dev_alloc(&h->pending, (size_t)(sites / g.ncol + 1)))) return bail(rc);
+        if ((rc = dev_alloc(&h->pending_count, 1))) return bail(rc);
+        if (cudaMemset(h->pending_count, 0, sizeof(int))) return bail(fail(GLZ_DRIVER, "memset failed"));
     }
     if ((rc = dev_alloc(&h->error_flag, 1))) return bail(rc);
     if ((rc = dev_alloc(&h->medium, 2))) return bail(rc);
@@ -837,7 +868,8 @@ void glz_gpu_destroy(glz_gpu *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->contact); cudaFree(h->tv); cudaFree(h->lv); cudaFree(h->ts); cudaFree(h->ls);
-    cudaFree(h->chemo); cudaFree(h->sec); cudaFree(h->upt); cudaFree(h->ext);
+    cudaFree(h->chemo); cudaFree(h->sec); cudaFree(h->upt); cudaFree(h->ext); cudaFree(h->maxact); cudaFree(h->lamact);
+    cudaFree(h->activity); cudaFree(h->pending); cudaFree(h->pending_count);
     cudaFree(h->tl); cudaFree(h->ll); cudaFree(h->divv); cudaFree(h->death); cudaFree(h->connected);
     cudaFree(h->labels); cudaFree(h->cell_type); cudaFree(h->field_buf); cudaFree(h->dose);
     cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->counters);

@@ -32,6 +32,7 @@ struct TypeTables {
     const uint8_t *connected;
     const float *chemotaxis, *secretion, *uptake;  // n_types * n_species
     const float *external;                         // n_types * 3: the drift vector
+    const float *max_activity, *lambda_activity;   // the motility (Act) term
 };
 
 // The per-cell tallies a colour pass reads, in the rotation that gives every
@@ -78,7 +79,14 @@ struct SweepLaunch {
     int uniform_contact_exact;  // J m is exact in f32 for every |m| <= n_off (see sweep.cu)
     float uniform_contact;      // J[type][type] when uniform
     float u_target_volume, u_lambda_volume, u_target_surface, u_lambda_surface;
-    int has_length, tracks, has_chemotaxis, has_external;
+    int has_length, tracks, has_chemotaxis, has_external, has_motility;
+    // Motility reads labels and activity two sites from the target, where
+    // same-colour targets change during the pass, so a pass with it leaves
+    // both as they were and lists its accepted copies (target, new label)
+    // for launch_apply_copies.
+    const float *activity;
+    uint2 *pending;
+    int *pending_count;
     const float *fields[kMaxSpecies];
     int use_tma;
     int lean;                // take the lean kernel: no length, chemotaxis, connectivity or moment tracking
@@ -88,6 +96,14 @@ struct SweepLaunch {
 };
 
 cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream);
+
+// Apply a motility pass's listed copies: the label, and the activity of a
+// type with a maximum (lib.rs:696-698); then clear the list.
+cudaError_t launch_apply_copies(const SweepLaunch &a, float *activity, cudaStream_t stream);
+
+// The activity's memory runs down by one each Monte Carlo step
+// (lib.rs:426-432, motility.rs).
+cudaError_t launch_activity_decay(float *activity, int sites, cudaStream_t stream);
 
 // The batched ensemble: independent replicas of one neighbourhood, all their
 // tiles in one persistent launch per colour. Replica state lives in flat

@@ -225,7 +225,31 @@ __device__ __forceinline__ void terms_of(const SweepLaunch &a, uint32_t label, i
     site_terms<DIM>(fold_int(x - an[0], a.g.w), fold_int(y - an[1], a.g.h), fold_int(z - an[2], a.g.d), t);
 }
 
-// The length and chemotaxis terms of a copy (cpu.rs:291-305, 381-395).
+// The geometric mean of the activity over the sites of `label` around `site`
+// (x, y, z), the site itself included; zero as soon as one of them has none
+// left (lib.rs:391-424, motility.rs:58-79). Labels and activity are the
+// pass's starting values: a pass with motility defers its writes.
+template <int DIM>
+__device__ __noinline__ float activity_mean(const SweepLaunch &a, uint32_t site, int x, int y, int z,
+                                            uint32_t label) {
+    const float here = a.activity[site];
+    if (!(here > 0.0f)) return 0.0f;
+    float log_sum = motility_log(here), count = 1.0f;
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    for (int k = 0; k < a.g.n_off; ++k) {
+        const uint32_t n = (uint32_t)(((size_t)wrap(z + a.g.off[k][2], D) * H + wrap(y + a.g.off[k][1], H)) * W +
+                                      wrap(x + a.g.off[k][0], W));
+        if (n == site || a.labels[n] != label) continue;
+        const float v = a.activity[n];
+        if (!(v > 0.0f)) return 0.0f;
+        log_sum = __fadd_rn(log_sum, motility_log(v));
+        count = __fadd_rn(count, 1.0f);
+    }
+    return metropolis_exp(__fdiv_rn(log_sum, count));
+}
+
+// The length, chemotaxis, motility and drift terms of a copy (cpu.rs:291-305,
+// 341-395).
 template <int DIM>
 __device__ __noinline__ float extra_terms(const SweepLaunch &a, uint32_t old, uint32_t nw, int t_old, int t_new,
                                           int vol_old, int vol_new, int x, int y, int z, int pick, uint32_t target,
@@ -252,6 +276,17 @@ __device__ __noinline__ float extra_terms(const SweepLaunch &a, uint32_t old, ui
             if (lam == 0.0f) continue;
             const float *f = a.fields[s];
             delta = __fsub_rn(delta, __fmul_rn(lam, __fsub_rn(f[target], f[source])));
+        }
+    }
+    // Motility (cpu.rs:346-352, lib.rs:656-663): the cell's memory pulls it
+    // where it has been.
+    if (a.has_motility && nw != 0) {
+        const float lam = a.t.lambda_activity[t_new], top = a.t.max_activity[t_new];
+        if (lam != 0.0f && top > 0.0f) {
+            const uint32_t source = (uint32_t)(((size_t)sz * H + sy) * W + sx);
+            const float into = activity_mean<DIM>(a, source, sx, sy, sz, nw);
+            const float out_of = activity_mean<DIM>(a, target, x, y, z, old);
+            delta = __fsub_rn(delta, __fmul_rn(__fdiv_rn(lam, top), __fsub_rn(into, out_of)));
         }
     }
     // The drift (cpu.rs:360-369, lib.rs:664-673): work e . (target - source),
@@ -408,7 +443,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const int
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
         }
     }
-    if (EXTRAS && (a.has_length || a.has_chemotaxis || a.has_external))
+    if (EXTRAS && (a.has_length || a.has_chemotaxis || a.has_external || a.has_motility))
         delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
 
     // Metropolis: a copy that lowers the energy (or keeps it) is taken, else
@@ -420,7 +455,12 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const int
         if (!(delta <= 0.0f || u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
     }
 
-    a.labels[target] = nw;
+    if (EXTRAS && a.has_motility) {
+        const int k = atomicAdd(a.pending_count, 1);
+        a.pending[k] = make_uint2(target, nw);
+    } else {
+        a.labels[target] = nw;
+    }
     if (old != 0) {
         atomicAdd(&a.vs_cur[old], pack_delta(-1, ds_old));
         atomicSub(&a.vol_by_colour[(size_t)old * a.g.ncol + a.colour], 1);
@@ -1047,6 +1087,38 @@ static cudaError_t launch_any(const SweepLaunch &a, cudaStream_t stream) {
         if (a.g.n_off == 26) return launch<3, 26, UNIFORM>(a, stream);
     }
     return cudaErrorInvalidValue;
+}
+
+__global__ void apply_copies_kernel(const __grid_constant__ SweepLaunch a, float *activity) {
+    const int count = *a.pending_count;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+        const uint2 p = a.pending[k];
+        a.labels[p.x] = p.y;
+        if (p.y != 0) {
+            const float top = a.t.max_activity[a.cell_type[p.y]];
+            if (top > 0.0f) activity[p.x] = top;
+        }
+    }
+}
+
+cudaError_t launch_apply_copies(const SweepLaunch &a, float *activity, cudaStream_t stream) {
+    // at most one copy per target, and a pass has sites / colours targets
+    const int most = a.g.sites / a.g.ncol + 1;
+    apply_copies_kernel<<<(most + 255) / 256, 256, 0, stream>>>(a, activity);
+    if (cudaError_t e = cudaGetLastError()) return e;
+    return cudaMemsetAsync(a.pending_count, 0, sizeof(int), stream);
+}
+
+__global__ void activity_decay_kernel(float *activity, int sites) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sites) return;
+    const float v = activity[i];
+    activity[i] = v > 0.0f ? __fsub_rn(v, 1.0f) : 0.0f;
+}
+
+cudaError_t launch_activity_decay(float *activity, int sites, cudaStream_t stream) {
+    activity_decay_kernel<<<(sites + 255) / 256, 256, 0, stream>>>(activity, sites);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream) {

@@ -93,6 +93,38 @@ EXPORT float rp_expf(float x) {
     return p * scale;
 }
 
+/* ln x for the motility term: 2 atanh((m - 1) / (m + 1)) as the series
+ * s + s^3/3 + ... + s^9/9 (Abramowitz and Stegun 4.1.27) on the mantissa m
+ * reduced to [sqrt(1/2), sqrt(2)], plus e ln 2 split hi + lo; the device's
+ * operations in the same order. */
+EXPORT float rp_logf(float x) {
+    int e = 0;
+    if (x < 1.17549435e-38f) {
+        x = x * 16777216.0f;
+        e = -24;
+    }
+    uint32_t bits;
+    memcpy(&bits, &x, sizeof bits);
+    e += (int)((bits >> 23) & 0xff) - 127;
+    uint32_t mb = (bits & 0x007fffffu) | 0x3f800000u;
+    float m;
+    memcpy(&m, &mb, sizeof m);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    float s = (m - 1.0f) / (m + 1.0f);
+    float s2 = s * s;
+    float p = 0.111111111f;
+    p = fmaf(p, s2, 0.142857143f);
+    p = fmaf(p, s2, 0.2f);
+    p = fmaf(p, s2, 0.333333333f);
+    p = p * s2;
+    float lm = (2.0f * s) * (1.0f + p);
+    float fe = (float)e;
+    return fmaf(fe, 0.693145751953125f, lm) + fe * 1.428606765330187e-06f;
+}
+
 /* ---------------------------------------------------------------- geometry */
 
 static inline int wrapi(int v, int n) {
@@ -165,6 +197,11 @@ typedef struct {
     float *contact, *tv, *lv, *ts, *ls, *chemo, *sec, *upt;
     float *ext; /* 3 per type: the drift vector */
     int has_external;
+    /* motility (Act): activity per site, per-type maximum and strength; a
+     * pass with it lists its copies and applies them at its end */
+    float *maxact, *lamact, *act;
+    int has_motility;
+    uint32_t *pending; /* 2 per copy: target, new label */
     double *tl, *ll, *div_vol, *death;
     uint8_t *connected;
     float *fd, *fdecay; /* per species per sub-step */
@@ -307,6 +344,9 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
     s->death = f64_copy(m->death_rate, nt);
     s->chemo = f32_copy(m->chemotaxis, (size_t)nt * ns);
     s->ext = f32_copy(m->external, 3 * (size_t)nt);
+    s->maxact = f32_copy(m->max_activity, (size_t)nt);
+    s->lamact = f32_copy(m->lambda_activity, (size_t)nt);
+    for (int t = 0; t < nt; ++t) s->has_motility |= s->lamact[t] != 0.0f && s->maxact[t] > 0.0f;
     for (int i = 0; i < 3 * nt; ++i) s->has_external |= s->ext[i] != 0.0f;
     s->sec = f32_copy(m->secretion, (size_t)nt * ns);
     s->upt = f32_copy(m->uptake, (size_t)nt * ns);
@@ -346,6 +386,8 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
     s->n_labels = n_labels;
     reserve(s, n_labels);
     memcpy(s->cell_type, cell_type, n_labels);
+    s->act = (float *)calloc((size_t)s->sites, sizeof(float));
+    s->pending = (uint32_t *)malloc(2 * (size_t)s->sites * sizeof(uint32_t));
     s->fields = (float *)calloc((size_t)(ns ? ns : 1) * s->sites, sizeof(float));
     s->scratch = (float *)calloc((size_t)(ns ? ns : 1) * s->sites, sizeof(float));
     for (int k = 0; k < ns; ++k)
@@ -360,6 +402,7 @@ EXPORT void rp_destroy(rsim *s) {
     if (!s) return;
     free(s->contact); free(s->tv); free(s->lv); free(s->ts); free(s->ls); free(s->tl); free(s->ll);
     free(s->div_vol); free(s->death); free(s->chemo); free(s->sec); free(s->upt); free(s->ext); free(s->connected);
+    free(s->maxact); free(s->lamact); free(s->act); free(s->pending);
     free(s->fd); free(s->fdecay); free(s->substeps);
     free(s->dose);
     free(s->labels); free(s->cell_type); free(s->vol); free(s->surf); free(s->volc); free(s->anchor);
@@ -450,6 +493,25 @@ static double length_delta(const rsim *s, int t, int64_t n, const int64_t *m, co
 
 /* One colour pass over the lattice: every target of the colour, each priced
  * against the tallies at the start of the pass. */
+/* The geometric mean of the activity over the sites of `label` around `site`,
+ * the site itself included; zero once one of them has none left
+ * (lib.rs:391-424, motility.rs:58-79). */
+static float activity_mean(const rsim *s, int site, int x, int y, int z, uint32_t label) {
+    float here = s->act[site];
+    if (!(here > 0.0f)) return 0.0f;
+    float log_sum = rp_logf(here), count = 1.0f;
+    for (int k = 0; k < s->n_off; ++k) {
+        int n = (wrapi(z + s->off[k][2], s->d) * s->h + wrapi(y + s->off[k][1], s->h)) * s->w +
+                wrapi(x + s->off[k][0], s->w);
+        if (n == site || s->labels[n] != label) continue;
+        float v = s->act[n];
+        if (!(v > 0.0f)) return 0.0f;
+        log_sum = log_sum + rp_logf(v);
+        count = count + 1.0f;
+    }
+    return rp_expf(log_sum / count);
+}
+
 static void pass(rsim *s, int colour) {
     size_t n = s->n_labels;
     int32_t *snap_vol = (int32_t *)malloc(n * sizeof(int32_t));
@@ -460,6 +522,7 @@ static void pass(rsim *s, int colour) {
     memcpy(snap_mom, s->mom, n * s->nm * sizeof(int64_t));
 
     int32_t step = (int32_t)s->mcs;
+    size_t np = 0; /* copies listed for the end of the pass (motility) */
     int hw = s->w / 2, hh = s->h / 2, hd = s->dim == 3 ? s->d / 2 : 1;
     int cx = colour & 1, cy = (colour >> 1) & 1, cz = (colour >> 2) & 1;
     for (int iz = 0; iz < hd; ++iz)
@@ -561,6 +624,12 @@ static void pass(rsim *s, int colour) {
                         delta = delta - lam * (f[target] - f[source]);
                     }
                 }
+                /* motility, cpu.rs:346-352 */
+                if (nw != 0 && s->has_motility && s->lamact[t_new] != 0.0f && s->maxact[t_new] > 0.0f) {
+                    float into = activity_mean(s, (int)source, sx, sy, sz, nw);
+                    float out_of = activity_mean(s, (int)target, x, y, z, old);
+                    delta = delta - (s->lamact[t_new] / s->maxact[t_new]) * (into - out_of);
+                }
                 /* the drift, cpu.rs:360-369: work e . (target - source), folded */
                 if (nw != 0 && s->has_external) {
                     float ex = s->ext[3 * t_new], ey = s->ext[3 * t_new + 1], ez = s->ext[3 * t_new + 2];
@@ -578,7 +647,14 @@ static void pass(rsim *s, int colour) {
                 }
                 if (!accept) continue;
                 s->accepted += 1;
-                s->labels[target] = nw;
+                if (s->has_motility) {
+                    /* motility reads two sites out: the pass's writes wait */
+                    s->pending[2 * np] = target;
+                    s->pending[2 * np + 1] = nw;
+                    ++np;
+                } else {
+                    s->labels[target] = nw;
+                }
                 if (old != 0) {
                     s->vol[old] -= 1;
                     s->surf[old] += ds_old;
@@ -594,6 +670,11 @@ static void pass(rsim *s, int colour) {
                         for (int k = 0; k < s->nm; ++k) s->mom[nw * s->nm + k] += terms_new[k];
                 }
             }
+    for (size_t k = 0; k < np; ++k) {
+        uint32_t target = s->pending[2 * k], nw = s->pending[2 * k + 1];
+        s->labels[target] = nw;
+        if (nw != 0 && s->maxact[s->cell_type[nw]] > 0.0f) s->act[target] = s->maxact[s->cell_type[nw]];
+    }
     free(snap_vol);
     free(snap_surf);
     free(snap_mom);
@@ -781,6 +862,8 @@ EXPORT int rp_set_infection(rsim *s, int species, int from_type, int to_type, do
 EXPORT void rp_step(rsim *s, uint64_t steps) {
     for (uint64_t r = 0; r < steps; ++r) {
         for (int c = 0; c < s->ncol; ++c) pass(s, c);
+        if (s->has_motility)
+            for (int i = 0; i < s->sites; ++i) s->act[i] = s->act[i] > 0.0f ? s->act[i] - 1.0f : 0.0f;
         if (s->n_species > 0) field_step(s);
         if (s->inf_species >= 0)
             for (size_t l = 1; l < s->n_labels; ++l)

@@ -62,7 +62,7 @@ def test_an_odd_side_is_refused_with_the_reference_message(L):
     assert "even sides" in _lib.last_error()
 
 
-@pytest.mark.parametrize("term", ["nematic", "motility"])
+@pytest.mark.parametrize("term", ["nematic"])
 def test_a_term_the_engine_does_not_run_is_refused(L, term):
     m = sheet_model(width=32, height=32)
     if term == "nematic":

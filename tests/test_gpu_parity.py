@@ -111,6 +111,12 @@ def _drift():
     return tiled(m, 8, 6, 6), 25
 
 
+def _motility():
+    # Act: a strong memory (max 20, lambda 60), writes deferred to the pass's end
+    m = sheet_model(seed=17, max_activity=20.0, lambda_activity=60.0, target_volume=64.0)
+    return tiled(m, 8, 5, 5), 25
+
+
 def _population():
     m = sheet_model(seed=8, division_volume=72.0, death_rate=0.005, target_volume=100.0)
     return tiled(m, 6, 6, 6), 40
@@ -146,6 +152,7 @@ CASES = {
     "connected": _connected,
     "population": _population,
     "drift": _drift,
+    "motility": _motility,
     "chemotaxis-ramp": _chemotaxis_ramp,
 }
 

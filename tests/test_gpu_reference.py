@@ -253,3 +253,19 @@ def test_the_device_drifts_a_cell_the_way_it_points(device, sign):
     gpu.close()
     assert sign * (x1 - x0) > 5.0, f"the cell moved {x1 - x0} along x"
     assert abs(y1 - y0) < 4.0, f"the cell wandered {y1 - y0} across the drift"
+
+
+def test_the_device_makes_a_cell_travel_on_its_memory(device):
+    # motility.rs:181-197: over 400 MCS a cell with a memory (max 20, lambda 60)
+    # travels more than three times as far as a plain one
+    def travelled(max_activity, lambda_activity):
+        st = _lone_cell(_motility_model(max_activity, lambda_activity, (0.0, 0.0, 0.0), False))
+        x0, y0 = _centroid(st.labels, 96)
+        gpu = device.GpuSimulation.from_start(st)
+        gpu.step(400)
+        x1, y1 = _centroid(gpu.labels(), 96)
+        gpu.close()
+        return math.hypot(x1 - x0, y1 - y0)
+
+    still, motile = travelled(0.0, 0.0), travelled(20.0, 60.0)
+    assert motile > 3.0 * still, f"a motile cell went {motile} on the device against {still} for a plain one"

@@ -182,3 +182,21 @@ def test_the_infection_rule_spreads_and_only_from_healthy_cells():
         r.set_infection(2, 1, 2, 5.0)
     with pytest.raises(ValueError):
         r.set_infection(0, 1, 2, 1e12)  # past the fixed-point range
+
+
+def test_the_motility_log_is_within_two_ulps_of_libm():
+    """The motility term's own log (the atanh series) against the C library's,
+    over the activity values a run can hold and a spread of positive floats."""
+    import ctypes as C
+
+    L = R.lib()
+    L.rp_logf.argtypes = [C.c_float]
+    L.rp_logf.restype = C.c_float
+    xs = np.concatenate([np.arange(1, 101, dtype=np.float32),
+                         np.float32(2.0) ** np.random.default_rng(5).uniform(-30, 30, 4000).astype(np.float32),
+                         np.float32([0.5, 0.75, 1.41421, 1.41422, 1e-40, 3.4e38])])
+    for x in xs:
+        got = np.float32(L.rp_logf(float(x)))
+        want = np.float32(math.log(float(x)))
+        ulp = np.spacing(np.abs(want)) if want != 0 else np.float32(1e-45)
+        assert abs(float(got) - float(want)) <= 2 * float(ulp) + 1e-7 * (abs(float(want)) < 1e-3), (x, got, want)
