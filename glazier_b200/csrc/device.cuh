@@ -98,6 +98,30 @@ __device__ __forceinline__ float motility_log(float x) {
     return __fadd_rn(__fmaf_rn(fe, 0.693145751953125f, lm), __fmul_rn(fe, 1.428606765330187e-06f));
 }
 
+// A nematic field component in the per-cell sums, in units of 2^-32 rounded
+// to nearest: the sums are exact and their order does not matter.
+__device__ __forceinline__ long long nematic_fixed(float q) { return __double2ll_rn((double)q * 4294967296.0); }
+
+// In-plane anisotropy ((c_xx - c_yy), 2 c_xy) / (c_xx + c_yy) of a cell of n
+// sites from its exact moment sums (moments.rs anisotropy; the quantity the
+// nematic term dots with the field): zero below two sites or for a vanishing
+// trace.
+template <int DIM>
+__device__ __forceinline__ void anisotropy(long long n, const long long *m, double &a0, double &a1) {
+    a0 = 0.0;
+    a1 = 0.0;
+    if (n < 2) return;
+    const double dn = (double)n;
+    const double mx = (double)m[0] / dn, my = (double)m[1] / dn;
+    const double cxx = (double)m[DIM == 2 ? 2 : 3] / dn - mx * mx;
+    const double cyy = (double)m[DIM == 2 ? 3 : 4] / dn - my * my;
+    const double cxy = (double)m[DIM == 2 ? 4 : 6] / dn - mx * my;
+    const double trace = cxx + cyy;
+    if (!(trace > 1e-12)) return;
+    a0 = (cxx - cyy) / trace;
+    a1 = 2.0 * cxy / trace;
+}
+
 __host__ __device__ __forceinline__ int wrap(int v, int n) {
     int r = v % n;
     return r < 0 ? r + n : r;

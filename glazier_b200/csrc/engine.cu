@@ -110,7 +110,8 @@ struct glz_gpu {
     float beta = 0.0f;
     uint64_t seed = 0;
     bool has_length = false, tracks = false, has_chemotaxis = false, has_pop = false, has_external = false;
-    bool has_motility = false;
+    bool has_motility = false, has_nematic = false;
+    float *nematic = nullptr;  // 2 per site, with the nematic term
     float *activity = nullptr;  // sites, with motility
     uint2 *pending = nullptr;   // a motility pass's accepted copies
     int *pending_count = nullptr;
@@ -120,7 +121,7 @@ struct glz_gpu {
     // per-type tables
     float *contact = nullptr, *tv = nullptr, *lv = nullptr, *ts = nullptr, *ls = nullptr;
     float *chemo = nullptr, *sec = nullptr, *upt = nullptr, *ext = nullptr, *maxact = nullptr, *lamact = nullptr;
-    double *tl = nullptr, *ll = nullptr, *divv = nullptr, *death = nullptr;
+    double *tl = nullptr, *ll = nullptr, *divv = nullptr, *death = nullptr, *lnem = nullptr;
     uint8_t *connected = nullptr;
 
     // state
@@ -172,6 +173,7 @@ struct glz_gpu {
         tt.external = ext;
         tt.max_activity = maxact;
         tt.lambda_activity = lamact;
+        tt.lambda_nematic = lnem;
         tt.secretion = sec;
         tt.uptake = upt;
         return tt;
@@ -293,6 +295,7 @@ int recount(glz_gpu *h) {
     r.vol_by_colour = h->t.vol_by_colour;
     r.anchor = h->t.anchor;
     r.tracks = h->tracks;
+    r.nematic = h->has_nematic ? h->nematic : nullptr;
     r.error_flag = h->error_flag;
     CU(glz::launch_recount(r, h->stream));
     return GLZ_OK;
@@ -369,6 +372,8 @@ int sweep_pass(glz_gpu *h, int colour) {
     a.has_chemotaxis = h->has_chemotaxis;
     a.has_external = h->has_external;
     a.has_motility = h->has_motility;
+    a.has_nematic = h->has_nematic;
+    a.nematic = h->nematic;
     a.activity = h->activity;
     a.pending = h->pending;
     a.pending_count = h->pending_count;
@@ -548,7 +553,6 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         motility |= at(m->lambda_activity, k) != 0.0 && at(m->max_activity, k) > 0.0;
         for (int a = 0; a < 3; ++a) drift |= at(m->external, 3 * (size_t)k + a) != 0.0;
     }
-    if (nematic) return fail(GLZ_UNSUPPORTED, "the device engine does not run the nematic term");
     if (activity && !motility)
         for (long long i = 0; i < sites; ++i)
             if (activity[i] != 0.0) return fail(GLZ_UNSUPPORTED, "a nonzero activity needs the motility term");
@@ -575,7 +579,9 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     g.dim = d > 1 ? 3 : 2;
     g.ncol = g.dim == 3 ? 8 : 4;
     g.sites = (int)sites;
-    g.nm = g.dim == 3 ? 9 : 5;
+    // the moment words: the geometric sums, then the nematic field's two
+    h->has_nematic = nematic;
+    g.nm = (g.dim == 3 ? 9 : 5) + (nematic ? 2 : 0);
     g.n_off = offsets_for(m->neighbour_order, d, g.off);
     h->n_types = nt;
     h->n_species = ns;
@@ -601,7 +607,9 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         h->has_length |= ll[k] != 0.0;
         h->has_pop |= divv[k] > 0.0 || death[k] > 0.0;
     }
-    h->tracks = h->has_length || h->has_pop;
+    h->tracks = h->has_length || h->has_pop || h->has_nematic;
+    std::vector<double> lnem(nt);
+    for (int k = 0; k < nt; ++k) lnem[k] = at(m->lambda_nematic, k);
     std::vector<float> maxact(nt), lamact(nt);
     for (int k = 0; k < nt; ++k) {
         maxact[k] = (float)at(m->max_activity, k);
@@ -652,7 +660,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         (rc = upload(h, &h->ll, ll)) || (rc = upload(h, &h->divv, divv)) || (rc = upload(h, &h->death, death)) ||
         (rc = upload(h, &h->connected, conn)) || (rc = upload(h, &h->chemo, chemo)) || (rc = upload(h, &h->sec, sec)) ||
         (rc = upload(h, &h->upt, upt)) || (rc = upload(h, &h->ext, ext)) || (rc = upload(h, &h->maxact, maxact)) ||
-        (rc = upload(h, &h->lamact, lamact)))
+        (rc = upload(h, &h->lamact, lamact)) || (rc = upload(h, &h->lnem, lnem)))
         return bail(rc);
 
     if ((rc = dev_alloc(&h->labels, (size_t)sites))) return bail(rc);
@@ -671,6 +679,13 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
             if (cudaMemcpy(h->field_ptr(s, 0), f.data(), sites * sizeof(float), cudaMemcpyHostToDevice))
                 return bail(fail(GLZ_DRIVER, "field upload failed"));
         }
+    }
+    if (h->has_nematic) {
+        std::vector<float> q(2 * (size_t)sites);
+        for (size_t i = 0; i < q.size(); ++i) q[i] = (float)m->nematic[i];
+        if ((rc = dev_alloc(&h->nematic, q.size()))) return bail(rc);
+        if (cudaMemcpy(h->nematic, q.data(), q.size() * sizeof(float), cudaMemcpyHostToDevice))
+            return bail(fail(GLZ_DRIVER, "nematic field upload failed"));
     }
     if (h->has_motility) {
         std::vector<float> act((size_t)sites);
@@ -839,10 +854,17 @@ int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len) {
         std::snprintf(msg, sizeof msg, "nematic field has %zu sites, the lattice %d", len / 2, h->g.sites);
         return fail(GLZ_INVALID, msg);
     }
-    (void)field;
-    // Models with a nematic coupling are refused at creation, so no handle
-    // has one to update (lib.rs:1207-1210).
-    return fail(GLZ_UNSUPPORTED, "the model has no nematic coupling to update");
+    // lib.rs:1207-1210
+    if (!h->has_nematic) return fail(GLZ_DRIVER, "the model has no nematic coupling to update");
+    if (!field) return fail(GLZ_INVALID, "null field");
+    std::vector<float> q(len);
+    for (size_t i = 0; i < len; ++i) q[i] = (float)field[i];
+    CU(cudaMemcpyAsync(h->nematic, q.data(), len * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    // the per-cell sums follow the new field: settle, then recount every tally
+    if (int rc = settle(h)) return rc;
+    if (int rc = recount(h)) return rc;
+    CU(cudaStreamSynchronize(h->stream));
+    return GLZ_OK;
 }
 
 uint64_t glz_gpu_mcs(const glz_gpu *h) { return h ? h->mcs : 0; }
@@ -869,7 +891,7 @@ void glz_gpu_destroy(glz_gpu *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->contact); cudaFree(h->tv); cudaFree(h->lv); cudaFree(h->ts); cudaFree(h->ls);
     cudaFree(h->chemo); cudaFree(h->sec); cudaFree(h->upt); cudaFree(h->ext); cudaFree(h->maxact); cudaFree(h->lamact);
-    cudaFree(h->activity); cudaFree(h->pending); cudaFree(h->pending_count);
+    cudaFree(h->activity); cudaFree(h->pending); cudaFree(h->pending_count); cudaFree(h->nematic); cudaFree(h->lnem);
     cudaFree(h->tl); cudaFree(h->ll); cudaFree(h->divv); cudaFree(h->death); cudaFree(h->connected);
     cudaFree(h->labels); cudaFree(h->cell_type); cudaFree(h->field_buf); cudaFree(h->dose);
     cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->counters);

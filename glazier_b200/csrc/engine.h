@@ -33,6 +33,7 @@ struct TypeTables {
     const float *chemotaxis, *secretion, *uptake;  // n_types * n_species
     const float *external;                         // n_types * 3: the drift vector
     const float *max_activity, *lambda_activity;   // the motility (Act) term
+    const double *lambda_nematic;
 };
 
 // The per-cell tallies a colour pass reads, in the rotation that gives every
@@ -79,7 +80,10 @@ struct SweepLaunch {
     int uniform_contact_exact;  // J m is exact in f32 for every |m| <= n_off (see sweep.cu)
     float uniform_contact;      // J[type][type] when uniform
     float u_target_volume, u_lambda_volume, u_target_surface, u_lambda_surface;
-    int has_length, tracks, has_chemotaxis, has_external, has_motility;
+    int has_length, tracks, has_chemotaxis, has_external, has_motility, has_nematic;
+    // the nematic field, (Q_xx, Q_xy) per site; its per-cell sums ride in the
+    // moment words after the geometric ones (g.nm counts both)
+    const float *nematic;
     // Motility reads labels and activity two sites from the target, where
     // same-colour targets change during the pass, so a pass with it leaves
     // both as they were and lists its accepted copies (target, new label)
@@ -186,6 +190,7 @@ struct RecountLaunch {
     int *vol_by_colour;
     int *anchor;
     int tracks;
+    const float *nematic;  // with the nematic term: its sums follow the moments
     int *error_flag;  // set to 2 when a label is not below n_labels
 };
 

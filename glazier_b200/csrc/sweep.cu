@@ -154,16 +154,41 @@ template <int DIM>
 __device__ __noinline__ double length_delta(const SweepLaunch &a, int type, int label, long long n,
                                             const long long *terms, int sign) {
     constexpr int NM = DIM == 2 ? 5 : 9;
+    const size_t at = (size_t)label * a.g.nm;  // the moment words of a cell: NM, then the nematic sums
     long long m[NM], after[NM];
 #pragma unroll
     for (int k = 0; k < NM; ++k) {
-        m[k] = a.mom_base[(size_t)label * NM + k] + a.mom_prev[(size_t)label * NM + k];
+        m[k] = a.mom_base[at + k] + a.mom_prev[at + k];
         after[k] = m[k] + sign * terms[k];
     }
     double tl = a.t.target_length[type];
     double before = axis_length<DIM>(n, m) - tl;
     double now = axis_length<DIM>(n + sign, after) - tl;
     return a.t.lambda_length[type] * (now * now - before * before);
+}
+
+// Change in a cell's nematic energy (cpu.rs:315-332, lib.rs:603-637) when the
+// site with sum terms `terms` (its moment terms, then its field components in
+// fixed point) leaves (sign -1) or joins (+1) it: -lambda (f' . a' - f . a),
+// f the cell's field sum and a its anisotropy, from the pass snapshot.
+template <int DIM>
+__device__ __noinline__ double nematic_delta(const SweepLaunch &a, int type, int label, long long n,
+                                             const long long *terms, int sign) {
+    constexpr int NM = DIM == 2 ? 5 : 9;
+    const size_t at = (size_t)label * a.g.nm;
+    long long m[NM + 2], after[NM + 2];
+#pragma unroll
+    for (int k = 0; k < NM + 2; ++k) {
+        m[k] = a.mom_base[at + k] + a.mom_prev[at + k];
+        after[k] = m[k] + sign * terms[k];
+    }
+    double a0, a1, b0, b1;
+    anisotropy<DIM>(n, m, a0, a1);
+    anisotropy<DIM>(n + sign, after, b0, b1);
+    const double scale = 1.0 / 4294967296.0;
+    const double before = (double)m[NM] * scale * a0 + (double)m[NM + 1] * scale * a1;
+    const double now = (double)after[NM] * scale * b0 + (double)after[NM + 1] * scale * b1;
+    return -a.t.lambda_nematic[type] * (now - before);
 }
 
 // lib.rs:371-389: whether the ring positions in `present` are one piece.
@@ -256,15 +281,26 @@ __device__ __noinline__ float extra_terms(const SweepLaunch &a, uint32_t old, ui
                                           float delta) {
     constexpr int NM = DIM == 2 ? 5 : 9;
     const int W = a.g.w, H = a.g.h, D = a.g.d;
-    if (a.has_length) {
-        long long terms[NM];
-        if (old != 0 && a.t.lambda_length[t_old] != 0.0) {
-            terms_of<DIM>(a, old, x, y, z, terms);
-            delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_old, old, vol_old, terms, -1));
+    // the length and nematic terms, leaving cell first (lib.rs:578-639)
+    if (a.has_length || a.has_nematic) {
+        long long terms[NM + 2];
+        if (a.has_nematic) {
+            terms[NM] = nematic_fixed(a.nematic[2 * (size_t)target]);
+            terms[NM + 1] = nematic_fixed(a.nematic[2 * (size_t)target + 1]);
         }
-        if (nw != 0 && a.t.lambda_length[t_new] != 0.0) {
+        const bool len_old = a.has_length && a.t.lambda_length[t_old] != 0.0;
+        const bool nem_old = a.has_nematic && a.t.lambda_nematic[t_old] != 0.0;
+        if (old != 0 && (len_old || nem_old)) {
+            terms_of<DIM>(a, old, x, y, z, terms);
+            if (len_old) delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_old, old, vol_old, terms, -1));
+            if (nem_old) delta = __fadd_rn(delta, (float)nematic_delta<DIM>(a, t_old, old, vol_old, terms, -1));
+        }
+        const bool len_new = a.has_length && a.t.lambda_length[t_new] != 0.0;
+        const bool nem_new = a.has_nematic && a.t.lambda_nematic[t_new] != 0.0;
+        if (nw != 0 && (len_new || nem_new)) {
             terms_of<DIM>(a, nw, x, y, z, terms);
-            delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_new, nw, vol_new, terms, 1));
+            if (len_new) delta = __fadd_rn(delta, (float)length_delta<DIM>(a, t_new, nw, vol_new, terms, 1));
+            if (nem_new) delta = __fadd_rn(delta, (float)nematic_delta<DIM>(a, t_new, nw, vol_new, terms, 1));
         }
     }
     const int ox = a.g.off[pick][0], oy = a.g.off[pick][1], oz = a.g.off[pick][2];
@@ -305,16 +341,26 @@ __device__ __noinline__ float extra_terms(const SweepLaunch &a, uint32_t old, ui
 template <int DIM>
 __device__ __noinline__ void commit_moments(const SweepLaunch &a, uint32_t old, uint32_t nw, int x, int y, int z) {
     constexpr int NM = DIM == 2 ? 5 : 9;
-    long long terms[NM];
+    const int nm = a.g.nm;
+    long long terms[NM], q[2] = {0, 0};
+    if (a.has_nematic) {
+        const size_t site = ((size_t)z * a.g.h + y) * a.g.w + x;
+        q[0] = nematic_fixed(a.nematic[2 * site]);
+        q[1] = nematic_fixed(a.nematic[2 * site + 1]);
+    }
     if (old != 0) {
         terms_of<DIM>(a, old, x, y, z, terms);
 #pragma unroll
-        for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)old * NM + k], (unsigned long long)(-terms[k]));
+        for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)old * nm + k], (unsigned long long)(-terms[k]));
+        if (a.has_nematic)
+            for (int k = 0; k < 2; ++k) atomicAdd(&a.mom_cur[(size_t)old * nm + NM + k], (unsigned long long)(-q[k]));
     }
     if (nw != 0) {
         terms_of<DIM>(a, nw, x, y, z, terms);
 #pragma unroll
-        for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)nw * NM + k], (unsigned long long)terms[k]);
+        for (int k = 0; k < NM; ++k) atomicAdd(&a.mom_cur[(size_t)nw * nm + k], (unsigned long long)terms[k]);
+        if (a.has_nematic)
+            for (int k = 0; k < 2; ++k) atomicAdd(&a.mom_cur[(size_t)nw * nm + NM + k], (unsigned long long)q[k]);
     }
 }
 
@@ -443,7 +489,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const int
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
         }
     }
-    if (EXTRAS && (a.has_length || a.has_chemotaxis || a.has_external || a.has_motility))
+    if (EXTRAS && (a.has_length || a.has_chemotaxis || a.has_external || a.has_motility || a.has_nematic))
         delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
 
     // Metropolis: a copy that lowers the energy (or keeps it) is taken, else
@@ -629,7 +675,7 @@ __device__ __forceinline__ uint32_t wait_parity(unsigned long long *bar, uint32_
 // this pass reads what is written here (engine.h).
 template <int DIM>
 __device__ __forceinline__ void rotate_tallies(const SweepLaunch &a) {
-    constexpr int NM = DIM == 2 ? 5 : 9;
+    const int NM = a.g.nm;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x; l < (size_t)a.n_labels; l += stride) {
         int dv, ds;

@@ -189,6 +189,11 @@ __global__ void recount_moments_kernel(const __grid_constant__ RecountLaunch a) 
         atomicAdd(&m[7], (unsigned long long)(ux * uz));
         atomicAdd(&m[8], (unsigned long long)(uy * uz));
     }
+    if (a.nematic) {
+        const int g = a.g.dim == 2 ? 5 : 9;
+        atomicAdd(&m[g], (unsigned long long)nematic_fixed(a.nematic[2 * i]));
+        atomicAdd(&m[g + 1], (unsigned long long)nematic_fixed(a.nematic[2 * i + 1]));
+    }
 }
 
 cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream) {

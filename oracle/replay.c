@@ -202,6 +202,11 @@ typedef struct {
     float *maxact, *lamact, *act;
     int has_motility;
     uint32_t *pending; /* 2 per copy: target, new label */
+    /* the nematic field (2 per site) and its per-cell sums, carried in the
+     * moment words after the geometric ones in units of 2^-32 */
+    float *nem;
+    double *lnem;
+    int has_nematic, nmg; /* nmg: the geometric moment words, 5 or 9 */
     double *tl, *ll, *div_vol, *death;
     uint8_t *connected;
     float *fd, *fdecay; /* per species per sub-step */
@@ -249,6 +254,10 @@ static inline int colour_of(const rsim *s, int x, int y, int z) {
 /* The tallies a device recount builds from the lattice: volume, volume per
  * colour, unlike-bond surface, anchor (the cell's first site in scan order)
  * and the exact moment sums about it. The medium's entries are kept too. */
+/* A nematic field component in the per-cell sums: units of 2^-32, rounded
+ * to nearest. */
+static int64_t nematic_fixed(float q) { return (int64_t)llrint((double)q * 4294967296.0); }
+
 static void recount(rsim *s) {
     size_t n = s->n_labels;
     memset(s->vol, 0, n * sizeof(int32_t));
@@ -289,6 +298,10 @@ static void recount(rsim *s) {
             m[3] += ux * ux; m[4] += uy * uy; m[5] += uz * uz;
             m[6] += ux * uy; m[7] += ux * uz; m[8] += uy * uz;
         }
+        if (s->has_nematic) {
+            m[s->nmg] += nematic_fixed(s->nem[2 * i]);
+            m[s->nmg + 1] += nematic_fixed(s->nem[2 * i + 1]);
+        }
     }
 }
 
@@ -325,7 +338,8 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
     s->d = m->depth;
     s->dim = s->d > 1 ? 3 : 2;
     s->ncol = s->dim == 3 ? 8 : 4;
-    s->nm = s->dim == 3 ? 9 : 5;
+    s->nmg = s->dim == 3 ? 9 : 5;
+    s->nm = s->nmg;
     s->sites = s->w * s->h * s->d;
     s->n_off = offsets_for(m->neighbour_order, m->depth, s->off);
     int nt = m->n_types, ns = m->n_species;
@@ -347,6 +361,15 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
     s->maxact = f32_copy(m->max_activity, (size_t)nt);
     s->lamact = f32_copy(m->lambda_activity, (size_t)nt);
     for (int t = 0; t < nt; ++t) s->has_motility |= s->lamact[t] != 0.0f && s->maxact[t] > 0.0f;
+    s->lnem = (double *)calloc((size_t)nt, sizeof(double));
+    for (int t = 0; t < nt; ++t) {
+        s->lnem[t] = m->lambda_nematic ? m->lambda_nematic[t] : 0.0;
+        s->has_nematic |= m->nematic != NULL && s->lnem[t] != 0.0;
+    }
+    if (s->has_nematic) {
+        s->nm = s->nmg + 2;
+        s->nem = f32_copy(m->nematic, 2 * (size_t)s->sites);
+    }
     for (int i = 0; i < 3 * nt; ++i) s->has_external |= s->ext[i] != 0.0f;
     s->sec = f32_copy(m->secretion, (size_t)nt * ns);
     s->upt = f32_copy(m->uptake, (size_t)nt * ns);
@@ -357,7 +380,7 @@ EXPORT rsim *rp_create(const glz_model *m, const uint32_t *labels, const uint8_t
         s->has_length |= s->ll[t] != 0.0;
         s->has_pop |= s->div_vol[t] > 0.0 || s->death[t] > 0.0;
     }
-    s->tracks = s->has_length || s->has_pop;
+    s->tracks = s->has_length || s->has_pop || s->has_nematic;
     s->fd = (float *)calloc(ns ? ns : 1, sizeof(float));
     s->fdecay = (float *)calloc(ns ? ns : 1, sizeof(float));
     s->substeps = (int *)calloc(ns ? ns : 1, sizeof(int));
@@ -402,7 +425,7 @@ EXPORT void rp_destroy(rsim *s) {
     if (!s) return;
     free(s->contact); free(s->tv); free(s->lv); free(s->ts); free(s->ls); free(s->tl); free(s->ll);
     free(s->div_vol); free(s->death); free(s->chemo); free(s->sec); free(s->upt); free(s->ext); free(s->connected);
-    free(s->maxact); free(s->lamact); free(s->act); free(s->pending);
+    free(s->maxact); free(s->lamact); free(s->act); free(s->pending); free(s->nem); free(s->lnem);
     free(s->fd); free(s->fdecay); free(s->substeps);
     free(s->dose);
     free(s->labels); free(s->cell_type); free(s->vol); free(s->surf); free(s->volc); free(s->anchor);
@@ -484,11 +507,43 @@ static void site_terms(int dim, int64_t ux, int64_t uy, int64_t uz, int64_t *t) 
 /* Change in a cell's length energy when the site at offset u (in its own
  * frame) leaves (sign -1) or joins (+1) it (cpu.rs:291-305). */
 static double length_delta(const rsim *s, int t, int64_t n, const int64_t *m, const int64_t *terms, int sign) {
-    int64_t after[9];
+    int64_t after[11];
     for (int k = 0; k < s->nm; ++k) after[k] = m[k] + sign * terms[k];
     double before = axis_length(s->dim, n, m) - s->tl[t];
     double now = axis_length(s->dim, n + sign, after) - s->tl[t];
     return s->ll[t] * (now * now - before * before);
+}
+
+/* In-plane anisotropy of a cell from its exact sums (moments.rs), as the
+ * device takes it. */
+static void anisotropy(const rsim *s, int64_t n, const int64_t *m, double *a0, double *a1) {
+    *a0 = 0.0;
+    *a1 = 0.0;
+    if (n < 2) return;
+    double dn = (double)n;
+    double mx = (double)m[0] / dn, my = (double)m[1] / dn;
+    double cxx = (double)m[s->dim == 2 ? 2 : 3] / dn - mx * mx;
+    double cyy = (double)m[s->dim == 2 ? 3 : 4] / dn - my * my;
+    double cxy = (double)m[s->dim == 2 ? 4 : 6] / dn - mx * my;
+    double trace = cxx + cyy;
+    if (!(trace > 1e-12)) return;
+    *a0 = (cxx - cyy) / trace;
+    *a1 = 2.0 * cxy / trace;
+}
+
+/* Change in a cell's nematic energy (cpu.rs:315-332) when the site with sum
+ * terms `terms` (moment terms, then the field in fixed point) leaves (-1) or
+ * joins (+1) it. */
+static double nematic_delta(const rsim *s, int t, int64_t n, const int64_t *m, const int64_t *terms, int sign) {
+    int64_t after[11];
+    for (int k = 0; k < s->nm; ++k) after[k] = m[k] + sign * terms[k];
+    double a0, a1, b0, b1;
+    anisotropy(s, n, m, &a0, &a1);
+    anisotropy(s, n + sign, after, &b0, &b1);
+    double scale = 1.0 / 4294967296.0;
+    double before = (double)m[s->nmg] * scale * a0 + (double)m[s->nmg + 1] * scale * a1;
+    double now = (double)after[s->nmg] * scale * b0 + (double)after[s->nmg + 1] * scale * b1;
+    return -s->lnem[t] * (now - before);
 }
 
 /* One colour pass over the lattice: every target of the colour, each priced
@@ -597,7 +652,13 @@ static void pass(rsim *s, int colour) {
                     float e = (float)snap_surf[nw] - s->ts[t_new], dsf = (float)ds_new;
                     delta = delta + s->ls[t_new] * (dsf * (2.0f * e + dsf));
                 }
-                int64_t terms_old[9], terms_new[9];
+                int64_t terms_old[11], terms_new[11];
+                if (s->has_nematic) {
+                    int64_t q0 = nematic_fixed(s->nem[2 * (size_t)target]);
+                    int64_t q1 = nematic_fixed(s->nem[2 * (size_t)target + 1]);
+                    terms_old[s->nmg] = terms_new[s->nmg] = q0;
+                    terms_old[s->nmg + 1] = terms_new[s->nmg + 1] = q1;
+                }
                 if (s->tracks) {
                     if (old != 0) {
                         const int32_t *an = &s->anchor[3 * old];
@@ -610,11 +671,18 @@ static void pass(rsim *s, int colour) {
                                    fold_int(z - an[2], s->d), terms_new);
                     }
                 }
-                if (s->has_length) {
-                    if (old != 0 && s->ll[t_old] != 0.0)
+                /* length then nematic, leaving cell first (lib.rs:578-639) */
+                if (old != 0) {
+                    if (s->has_length && s->ll[t_old] != 0.0)
                         delta = delta + (float)length_delta(s, t_old, snap_vol[old], &snap_mom[old * s->nm], terms_old, -1);
-                    if (nw != 0 && s->ll[t_new] != 0.0)
+                    if (s->has_nematic && s->lnem[t_old] != 0.0)
+                        delta = delta + (float)nematic_delta(s, t_old, snap_vol[old], &snap_mom[old * s->nm], terms_old, -1);
+                }
+                if (nw != 0) {
+                    if (s->has_length && s->ll[t_new] != 0.0)
                         delta = delta + (float)length_delta(s, t_new, snap_vol[nw], &snap_mom[nw * s->nm], terms_new, 1);
+                    if (s->has_nematic && s->lnem[t_new] != 0.0)
+                        delta = delta + (float)nematic_delta(s, t_new, snap_vol[nw], &snap_mom[nw * s->nm], terms_new, 1);
                 }
                 if (nw != 0) {
                     for (int k = 0; k < s->n_species; ++k) {
@@ -856,6 +924,15 @@ EXPORT int rp_set_infection(rsim *s, int species, int from_type, int to_type, do
     s->inf_from = from_type;
     s->inf_to = to_type;
     s->inf_threshold = llround(threshold * 16777216.0);
+    return 0;
+}
+
+/* Replace the nematic field (2 per site) and recount its per-cell sums, as
+ * glz_gpu_set_nematic_field does. */
+EXPORT int rp_set_nematic_field(rsim *s, const double *field) {
+    if (!s->has_nematic) return 2;
+    for (int i = 0; i < 2 * s->sites; ++i) s->nem[i] = (float)field[i];
+    recount(s);
     return 0;
 }
 

@@ -37,6 +37,8 @@ def lib():
                      "rp_moments", "rp_lengths"):
             getattr(L, name).argtypes = [P, P]
         L.rp_field.argtypes = [P, C.c_int, P]
+        L.rp_set_nematic_field.argtypes = [P, P]
+        L.rp_set_nematic_field.restype = C.c_int
         L.rp_set_infection.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_double]
         L.rp_set_infection.restype = C.c_int
         L.rp_expf.argtypes = [C.c_float]
@@ -80,6 +82,15 @@ class ReplayOracle:
 
     def step(self, steps: int = 1) -> None:
         lib().rp_step(self.h, steps)
+
+    def set_nematic_field(self, pairs) -> None:
+        """Replace the nematic field, (Q_xx, Q_xy) per site."""
+        flat = np.ascontiguousarray(pairs, dtype=np.float64).reshape(-1)
+        if flat.size != 2 * self.sites:
+            raise ValueError("the nematic field is not two values per site")
+        self._keep.append(flat)
+        if lib().rp_set_nematic_field(self.h, _ptr(flat)):
+            raise ValueError("the model has no nematic coupling to update")
 
     def set_infection(self, species: int, from_type: int, to_type: int, threshold: float) -> None:
         """The infection rule of glz_gpu_set_infection, same arguments."""

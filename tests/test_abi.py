@@ -62,20 +62,22 @@ def test_an_odd_side_is_refused_with_the_reference_message(L):
     assert "even sides" in _lib.last_error()
 
 
-@pytest.mark.parametrize("term", ["nematic"])
-def test_a_term_the_engine_does_not_run_is_refused(L, term):
+def test_an_activity_without_the_motility_term_is_refused(L):
+    """Every term of the reference's model runs on the device; an activity
+    field for a model that never reads it is refused rather than dropped."""
+    import ctypes as C
+
     m = sheet_model(width=32, height=32)
-    if term == "nematic":
-        m.types[1].lambda_nematic = 1.0
-        m.nematic = np.zeros((m.sites, 2))
-    elif term == "motility":
-        m.types[1].lambda_activity = 10.0
-        m.types[1].max_activity = 20.0
-    else:
-        m.types[1].external = (1.0, 0.0, 0.0)
-    rc, h = _create(m)
+    start = tiled(m)
+    keep: list = []
+    gm = _lib.model_struct(m, keep)
+    lab = np.ascontiguousarray(start.labels, dtype=np.uint32)
+    ct = np.ascontiguousarray(start.cell_type, dtype=np.uint8)
+    act = np.ones(m.sites)
+    h = C.c_void_p()
+    rc = L.glz_gpu_create(C.byref(gm), _lib.ptr(lab), _lib.ptr(ct), ct.size, None, _lib.ptr(act), C.byref(h))
     assert rc == _lib.GLZ_UNSUPPORTED and not h.value
-    assert term.split()[0] in _lib.last_error() or "Act" in _lib.last_error()
+    assert "motility" in _lib.last_error()
 
 
 def test_a_label_past_the_type_table_is_refused(L):

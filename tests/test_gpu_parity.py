@@ -117,6 +117,20 @@ def _motility():
     return tiled(m, 8, 5, 5), 25
 
 
+def _nematic():
+    # a random director field the cells' long axes couple to (and a length
+    # term beside it, so both read the same moment words)
+    m = sheet_model(seed=19, lambda_nematic=3.0, target_length=10.0, lambda_length=0.5)
+    m.nematic = np.random.default_rng(19).uniform(-0.5, 0.5, size=(m.sites, 2))
+    return tiled(m), 20
+
+
+def _nematic_volume():
+    m = sheet_model(width=32, height=32, depth=32, seed=20, target_volume=512.0, order=3, lambda_nematic=40.0)
+    m.nematic = np.random.default_rng(20).uniform(-1.0, 1.0, size=(m.sites, 2))
+    return tiled(m), 4
+
+
 def _population():
     m = sheet_model(seed=8, division_volume=72.0, death_rate=0.005, target_volume=100.0)
     return tiled(m, 6, 6, 6), 40
@@ -153,6 +167,8 @@ CASES = {
     "population": _population,
     "drift": _drift,
     "motility": _motility,
+    "nematic": _nematic,
+    "nematic-volume": _nematic_volume,
     "chemotaxis-ramp": _chemotaxis_ramp,
 }
 
@@ -227,3 +243,22 @@ def test_a_bad_infection_rule_is_refused(device):
         with pytest.raises(GpuError):
             gpu.set_infection(*rule)
     gpu.close()
+
+
+def test_a_replaced_nematic_field_reproduces_the_replay_bit_for_bit(device):
+    """glz_gpu_set_nematic_field mid-run: the per-cell sums follow the new
+    field on both sides."""
+    start, steps = _nematic()
+    gpu = device.GpuSimulation.from_start(start)
+    replay = ReplayOracle.from_start(start)
+    gpu.step(5)
+    replay.step(5)
+    field = np.random.default_rng(7).uniform(-1.0, 1.0, size=(start.model.sites, 2))
+    gpu.set_nematic_field(field)
+    replay.set_nematic_field(field)
+    gpu.step(10)
+    replay.step(10)
+    assert np.array_equal(gpu.labels(), replay.labels())
+    assert np.array_equal(gpu.volumes(), replay.volumes())
+    gpu.close()
+

@@ -269,3 +269,89 @@ def test_the_device_makes_a_cell_travel_on_its_memory(device):
 
     still, motile = travelled(0.0, 0.0), travelled(20.0, 60.0)
     assert motile > 3.0 * still, f"a motile cell went {motile} on the device against {still} for a plain one"
+
+
+def _nematic_model(lambda_nematic, angle):
+    # gpu_nematic.rs:16-36
+    from glazier_b200.blueprint import CellType, Model
+
+    m = Model(width=64, height=64, contact=[0.0, 16.0, 16.0, 8.0],
+              types=[CellType(), CellType(target_volume=64.0, lambda_volume=2.0, lambda_nematic=lambda_nematic)],
+              temperature=10.0, neighbour_order=2, seed=7)
+    m.nematic = np.tile([math.cos(2 * angle), math.sin(2 * angle)], (64 * 64, 1))
+    return m
+
+
+def _order(labels, width, height):
+    """gpu_nematic.rs:38-58: the nematic order |<exp(2 i theta)>| of the cells'
+    long axes and their mean director, over cells of eight sites or more."""
+    labels = np.asarray(labels).reshape(height, width)
+    c = s = n = 0.0
+    for l in np.unique(labels[labels > 0]):
+        ys, xs = np.nonzero(labels == l)
+        if xs.size < 8:
+            continue
+        # the cell's frame: minimum image about its first site
+        x0, y0 = xs[0], ys[0]
+        ux = (xs - x0 + width // 2) % width - width // 2
+        uy = (ys - y0 + height // 2) % height - height // 2
+        cxx, cyy = ux.var(), uy.var()
+        cxy = (ux * uy).mean() - ux.mean() * uy.mean()
+        trace = cxx + cyy
+        if trace <= 1e-12:
+            continue
+        a0, a1 = (cxx - cyy) / trace, 2 * cxy / trace
+        norm = math.hypot(a0, a1)
+        if norm < 1e-9:
+            continue
+        c += a0 / norm
+        s += a1 / norm
+        n += 1
+    return math.hypot(c, s) / n, 0.5 * math.atan2(s, c)
+
+
+def test_the_device_aligns_cells_along_the_field_as_the_serial_engine_does(device):
+    # gpu_nematic.rs:74-105
+    angle, steps = 0.6, 400
+    coupled = _nematic_model(6.0, angle)
+    gpu = device.GpuSimulation.from_start(tiled(coupled, 8))
+    gpu.step(steps)
+    s_gpu, director = _order(gpu.labels(), 64, 64)
+    gpu.close()
+    s_cpu, _ = _order(_serial(coupled, steps, tiled(coupled, 8)).labels(), 64, 64)
+    off = min(abs(director - angle), math.pi - abs(director - angle))
+    assert s_gpu > 0.7, f"device order {s_gpu}"
+    assert off < 0.15, f"device director {director} against the field's {angle}"
+    assert abs(s_gpu - s_cpu) < 0.15, f"device {s_gpu} against serial {s_cpu}"
+    blind = _nematic_model(0.0, angle)
+    gpu = device.GpuSimulation.from_start(tiled(blind, 8))
+    gpu.step(steps)
+    s_blind, _ = _order(gpu.labels(), 64, 64)
+    gpu.close()
+    assert s_blind < 0.4, f"uncoupled device order {s_blind}"
+
+
+def test_a_replaced_field_turns_the_cells_on_the_device(device):
+    # gpu_nematic.rs:107-131
+    from glazier_b200.engine import GpuError
+
+    first = 0.2
+    second = first + math.pi / 2
+    coupled = _nematic_model(6.0, first)
+    gpu = device.GpuSimulation.from_start(tiled(coupled, 8))
+    gpu.step(400)
+    _, before = _order(gpu.labels(), 64, 64)
+    turned = np.tile([math.cos(2 * second), math.sin(2 * second)], (64 * 64, 1))
+    gpu.set_nematic_field(turned)
+    gpu.step(800)
+    s_after, after = _order(gpu.labels(), 64, 64)
+
+    def off(d, a):
+        return min(abs(d - a), math.pi - abs(d - a))
+
+    assert off(before, first) < 0.15, f"before {before}"
+    assert s_after > 0.7, f"order after the turn {s_after}"
+    assert off(after, second) < 0.15, f"after {after} against {second}"
+    with pytest.raises(GpuError):
+        gpu.set_nematic_field(turned[1:])
+    gpu.close()

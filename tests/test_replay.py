@@ -200,3 +200,24 @@ def test_the_motility_log_is_within_two_ulps_of_libm():
         want = np.float32(math.log(float(x)))
         ulp = np.spacing(np.abs(want)) if want != 0 else np.float32(1e-45)
         assert abs(float(got) - float(want)) <= 2 * float(ulp) + 1e-7 * (abs(float(want)) < 1e-3), (x, got, want)
+
+
+@pytest.mark.parametrize("name", ["nematic", "nematic-volume", "motility", "drift"])
+def test_each_extra_term_changes_the_run(name):
+    """On the replay, each term's parity case lands elsewhere without the
+    term, so a device that skipped the term could not match it."""
+    import copy
+
+    from test_gpu_parity import CASES
+
+    made, steps = CASES[name]()
+    start = made
+    plain = copy.deepcopy(start)
+    for t in plain.model.types:
+        t.lambda_nematic = 0.0
+        t.lambda_activity = 0.0
+        t.external = (0.0, 0.0, 0.0)
+    a, b = R.ReplayOracle.from_start(start), R.ReplayOracle.from_start(plain)
+    a.step(steps)
+    b.step(steps)
+    assert not np.array_equal(a.labels(), b.labels())
