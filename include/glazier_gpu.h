@@ -13,8 +13,9 @@
  *   - One handle owns one CUDA stream on one device. A handle is not safe to
  *     use from two threads at once (the reference `GpuSession` is
  *     `unsendable`); distinct handles are independent.
- *   - A model term the device engine does not run is refused at creation
- *     with GLZ_UNSUPPORTED, never dropped silently (lib.rs:819-821).
+ *   - A model input the device engine would not use (an activity field with
+ *     no motility term) is refused at creation with GLZ_UNSUPPORTED, never
+ *     dropped silently (lib.rs:819-821).
  */
 #ifndef GLAZIER_GPU_H
 #define GLAZIER_GPU_H
@@ -77,9 +78,12 @@ const char *glz_last_error(void);
  *   cell_type  n_labels types, index 0 the medium; n_labels > max label
  *   fields     NULL (each species starts at its `initial`) or
  *              n_species * sites concentrations, species-major
- *   activity   NULL; a nonzero activity needs the motility term, refused
- * Refuses odd sides (GLZ_ODD_LATTICE, lib.rs:816-818) and the nematic,
- * motility and drift terms (GLZ_UNSUPPORTED).
+ *   activity   NULL (every site starts with none) or sites values, the
+ *              motility term's memory; a nonzero one for a model without
+ *              the motility term is refused (GLZ_UNSUPPORTED)
+ * Refuses odd sides (GLZ_ODD_LATTICE, lib.rs:816-818). Every term of the
+ * model runs: contact, volume, surface, length, connectivity, chemotaxis,
+ * nematic, motility (Act) and drift, fields, division and death.
  */
 int glz_gpu_create(const glz_model *model, const uint32_t *labels, const uint8_t *cell_type, size_t n_labels,
                    const double *fields, const double *activity, glz_gpu **out);
@@ -132,8 +136,9 @@ int glz_gpu_cell_types(glz_gpu *h, uint8_t *out, size_t *count);
 int glz_gpu_set_infection(glz_gpu *h, int species, int from_type, int to_type, double threshold);
 
 /* Replace the nematic field, 2 * sites values: GpuSimulation::set_nematic_field
- * (lib.rs:1199-1221). A model without a nematic coupling is refused with the
- * reference's message. */
+ * (lib.rs:1199-1221); the per-cell field sums are recounted. A field of the
+ * wrong length is GLZ_INVALID; a model without a nematic coupling is refused
+ * with the reference's message (GLZ_DRIVER, as the reference's Driver). */
 int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len);
 
 /* Monte Carlo steps completed: `pub mcs` (lib.rs:805). */
