@@ -274,6 +274,86 @@ def infection_compare(mcs: int, cpu_mcs: int, device: int) -> dict:
                            "cores": 1, "kind": "port", "note": "same start, infection rule off (the reference has none)"}}
 
 
+# The reference's published device times (README.md:116-121, 206-210, 248-250;
+# RTX 5060 Laptop): plane sizes with bench.rs's model, and three blueprints.
+PUBLISHED_SIZES = {128: 0.002, 256: 0.002, 512: 0.007, 1024: 0.024, 2048: 0.097, 4096: 0.446}
+PUBLISHED_BLUEPRINTS = {"volume.json": (50, 0.092), "infection-volume.json": (60, 0.081),
+                        "infection-512.json": (200, 1.66)}
+
+
+def published_rows(device: int) -> dict:
+    """The reference's published rows on this engine: 100 MCS of bench.rs's
+    model (tiled 8 x 8 cells, contact [0,16,16,8], lambda_V 2, V_t 64, T 10,
+    Moore, seed 1; glazier/examples/bench.rs) at each plane size, and the
+    three blueprints' steps, each timed from a created engine to the end of
+    its steps on the host clock (what the reference's figures time) and on
+    the device (CUDA events)."""
+    import torch
+
+    from glazier_b200 import native
+    from glazier_b200.blueprint import CellType, Model, Start
+    from glazier_b200.engine import GpuSimulation
+
+    rows = {}
+    for size, published in PUBLISHED_SIZES.items():
+        m = Model(width=size, height=size, contact=[0.0, 16.0, 16.0, 8.0],
+                  types=[CellType(), CellType(target_volume=64.0, lambda_volume=2.0)], temperature=10.0,
+                  neighbour_order=2, seed=1)
+        # a first engine pays the process's one-time costs (module loading,
+        # kernel attributes); the timed one starts from its own start
+        warm = GpuSimulation.from_start(Start.tiled(m, 8), device=device)
+        warm.step(2)
+        warm.close()
+        sim = GpuSimulation.from_start(Start.tiled(m, 8), device=device)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ms = sim.step_profiled(100)
+        wall = time.perf_counter() - t
+        sim.close()
+        rows[f"{size}^2"] = {"mcs": 100, "wall_s": wall, "device_ms": sum(ms), "published_s": published,
+                             "site_updates_per_s": size * size * 100 / wall, "speedup": published / wall}
+    texts = json.loads((ROOT / "tests" / "golden" / "serial_reference.json").read_text())["parse"]
+    for name, (steps, published) in PUBLISHED_BLUEPRINTS.items():
+        session = native.GpuSession(texts[name]["text"])
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        ms = session.simulation.step_profiled(steps)
+        wall = time.perf_counter() - t
+        session.simulation.close()
+        rows[name] = {"mcs": steps, "wall_s": wall, "device_ms": sum(ms), "published_s": published,
+                      "speedup": published / wall}
+    return rows
+
+
+def volume_leg(mcs: int, device: int, peak: float) -> dict:
+    """The scaling configuration's volume: a periodic 128^3 lattice of 4096
+    cubic cells of side 8, 26 neighbours, J 10, lambda_V 1 at V_t 512,
+    lambda_S 0.2 at S_t 3176 (a cube's initial unlike-bond count), T 10, seed
+    1; `mcs` MCS after 3 of warm-up, L2 flushed before each, device time. Its
+    algorithmic bytes are 36 per site-update (8 passes x 4 B read + 4 B
+    written)."""
+    import torch
+
+    from glazier_b200.engine import GpuSimulation
+    from glazier_b200.workloads import initial_surface, monolayer
+
+    start = monolayer(128, depth=128, lambda_surface=0.2, target_surface=initial_surface(8, 3))
+    sim = GpuSimulation.from_start(start, device=device)
+    sim.step(3)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{device}")
+    sweep = 0.0
+    for _ in range(mcs):
+        flush.zero_()
+        torch.cuda.synchronize()
+        sweep += sim.step_profiled(1)[0]
+    sim.close()
+    sites = start.model.sites
+    rate = sites * mcs / (sweep / 1e3)
+    return {"lattice": "128^3", "cells": start.n_cells, "mcs": mcs, "sweep_ms_per_mcs": sweep / mcs,
+            "site_updates_per_s": rate, "bytes_per_site_update": 36,
+            "roofline_frac": rate * 36 / 1e9 / peak, "l2": "flushed before each MCS (the lattice is 8 MB)"}
+
+
 def cpu_baseline(size: int, seconds: float) -> dict:
     """The serial engine on one host core, a bounded sample of the same lattice."""
     from oracle.serial import SerialOracle
@@ -447,6 +527,9 @@ def run_ours(args) -> None:
     }
     if world == 1 and not args.no_ensemble:
         line["ensemble"] = ensemble_compare(100, torch.cuda.current_device())
+    if world == 1 and not args.no_published:
+        line["volume"] = volume_leg(20, torch.cuda.current_device(), peak)
+        line["published_rows"] = published_rows(torch.cuda.current_device())
     if world == 1 and not args.no_infection:
         line["infection"] = infection_compare(200, 20, torch.cuda.current_device())
     if world == 1 and not args.no_adjoint:
@@ -469,6 +552,7 @@ def main() -> None:
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-infection", action="store_true")
+    ap.add_argument("--no-published", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")

@@ -801,6 +801,7 @@ constexpr int kLeanStages = 3;
 #endif
 constexpr int kLeanWarps = GLZ_LEAN_WARPS;
 constexpr int kLeanThreads = 32 * kLeanWarps;
+constexpr int kRotate = 2;  // labels per thread whose rotation reads are copied in ahead
 
 template <int DIM>
 struct LeanSmem {
@@ -815,6 +816,9 @@ struct LeanSmem {
     int issued[kLeanStages];  // copies issued into the buffer
     alignas(8) unsigned long long full[kLeanStages];     // the buffer's copy has landed
     alignas(8) unsigned long long patched[kLeanStages];  // every warp has patched its rows
+    // the tally rotation's first kRotate labels per thread, copied in while the tiles run
+    alignas(16) int2 rot_base[2 * kLeanThreads];
+    alignas(16) long long rot_prev[2 * kLeanThreads];
 };
 
 // Tensor copies for every tile, edge tiles included: the lattice's rows are
@@ -850,6 +854,11 @@ __device__ __forceinline__ void lean_patch(const SweepLaunch &a, uint32_t *win, 
     using T = Tile<DIM>;
     const int W = a.g.w, H = a.g.h, D = a.g.d;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // Whether every window coordinate is at most one lattice span outside it
+    // (the halo reaches back no further than a span, the last tile's window
+    // no further than one span past the end), so one step wraps it.
+    const auto reach = [](int n, int t, int h) { return h <= n && ((n - 1) / t) * t + t + h <= 2 * n; };
+    const bool once = reach(W, T::TX, T::HX) && reach(H, T::TY, 1) && (DIM == 2 || reach(D, T::TZ, T::HZ));
     int lo = 0, hi = 0;  // window columns [lo, hi) lie inside the lattice
     if (copies) {
         lo = T::HX - x0 > 0 ? T::HX - x0 : 0;
@@ -859,12 +868,13 @@ __device__ __forceinline__ void lean_patch(const SweepLaunch &a, uint32_t *win, 
         const int py = r % T::PY, pz = r / T::PY;
         const int gy = y0 - 1 + py, gz = DIM == 3 ? z0 - T::HZ + pz : 0;
         const bool inside = copies && gy >= 0 && gy < H && gz >= 0 && gz < D;
-        const uint32_t *row = a.labels + ((size_t)(DIM == 3 ? wrap(gz, D) : 0) * H + wrap(gy, H)) * W;
+        const auto wr = [once](int v, int n) { return once ? (v < 0 ? v + n : (v >= n ? v - n : v)) : wrap(v, n); };
+        const uint32_t *row = a.labels + ((size_t)(DIM == 3 ? wr(gz, D) : 0) * H + wr(gy, H)) * W;
         uint32_t *dst = win + r * T::PX;
         const int n = inside ? lo + (T::PX - hi) : T::PX;
         for (int c = lane; c < n; c += 32) {
             const int px = inside && c >= lo ? hi + (c - lo) : c;
-            dst[px] = row[wrap(x0 - T::HX + px, W)];
+            dst[px] = row[wr(x0 - T::HX + px, W)];
         }
     }
 }
@@ -917,8 +927,24 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         for (int i = 0; i < kLeanStages && i < mine; ++i) lean_issue<DIM>(a, tmap, S, i, copies);
     }
-    // the rotation's loads overlap the first copies
-    rotate_tallies<DIM>(a);
+    // Tally rotation (no thread of this pass reads what it writes): the reads
+    // of each thread's first kRotate labels are copied into shared memory now
+    // and finished after the tiles, so their latency hides behind pricing.
+    const size_t rot_stride = (size_t)gridDim.x * blockDim.x;
+    const size_t rot_first = (size_t)blockIdx.x * blockDim.x + tid;
+#pragma unroll
+    for (int k = 0; k < kRotate; ++k) {
+        const size_t l = rot_first + k * rot_stride;
+        if (l < (size_t)a.n_labels) {
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(&S.rot_base[k * kLeanThreads + tid])),
+                         "l"(a.vs_base + l)
+                         : "memory");
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(&S.rot_prev[k * kLeanThreads + tid])),
+                         "l"(a.vs_prev + l)
+                         : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
     const bool small_types = a.n_types <= kSmemTypes;
     if (!UNIFORM && small_types)
         for (int k = tid; k < a.n_types * a.n_types; k += blockDim.x) S.contact[k] = a.t.contact[k];
@@ -983,6 +1009,7 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
                 for (int k = 0; k < kLeanStages; ++k)
                     if (S.issued[k] > 0) wait_parity(&S.full[k], (uint32_t)(S.issued[k] - 1) & 1u);
             }
+            asm volatile("cp.async.wait_all;" ::: "memory");
             return;
         }
 
@@ -1060,6 +1087,26 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
                                                         hx0, hy0, hz0, small_types);
         __syncwarp();
         lean_release<DIM>(a, tmap, S, mine - 1, mine, copies);
+    }
+    // finish the rotation: this thread's copied labels, then any past them
+    asm volatile("cp.async.wait_all;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < kRotate; ++k) {
+        const size_t l = rot_first + k * rot_stride;
+        if (l < (size_t)a.n_labels) {
+            int dv, ds;
+            unpack_delta(S.rot_prev[k * kLeanThreads + tid], dv, ds);
+            const int2 b = S.rot_base[k * kLeanThreads + tid];
+            a.vs_next_base[l] = make_int2(b.x + dv, b.y + ds);
+            a.vs_clear[l] = 0;
+        }
+    }
+    for (size_t l = rot_first + kRotate * rot_stride; l < (size_t)a.n_labels; l += rot_stride) {
+        int dv, ds;
+        unpack_delta(a.vs_prev[l], dv, ds);
+        const int2 b = a.vs_base[l];
+        a.vs_next_base[l] = make_int2(b.x + dv, b.y + ds);
+        a.vs_clear[l] = 0;
     }
 }
 
