@@ -26,6 +26,8 @@
 
 #include <cuda.h>
 
+#include <cstdlib>
+
 #include "device.cuh"
 #include "engine.h"
 #include "neighbours.cuh"
@@ -925,8 +927,21 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
             S.issued[k] = 0;
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        for (int i = 0; i < kLeanStages && i < mine; ++i) lean_issue<DIM>(a, tmap, S, i, copies);
     }
+    const bool small_types = a.n_types <= kSmemTypes;
+    if (!UNIFORM && small_types)
+        for (int k = tid; k < a.n_types * a.n_types; k += blockDim.x) S.contact[k] = a.t.contact[k];
+#pragma unroll
+    for (int k = 0; k < NOFF; ++k)
+        if (tid == k) S.woff[k] = window_offset<DIM, NOFF>(k);
+    // Everything above reads nothing the previous pass writes. Launched
+    // programmatically, this grid may have started before that pass ended:
+    // wait here for it to finish (its labels and tallies visible), then let
+    // the next pass's grid start its own prologue.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (tid == 0)
+        for (int i = 0; i < kLeanStages && i < mine; ++i) lean_issue<DIM>(a, tmap, S, i, copies);
     // Tally rotation (no thread of this pass reads what it writes): the reads
     // of each thread's first kRotate labels are copied into shared memory now
     // and finished after the tiles, so their latency hides behind pricing.
@@ -945,12 +960,6 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
         }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
-    const bool small_types = a.n_types <= kSmemTypes;
-    if (!UNIFORM && small_types)
-        for (int k = tid; k < a.n_types * a.n_types; k += blockDim.x) S.contact[k] = a.t.contact[k];
-#pragma unroll
-    for (int k = 0; k < NOFF; ++k)
-        if (tid == k) S.woff[k] = window_offset<DIM, NOFF>(k);
     __syncthreads();
 
     // this lane's targets: offset from the tile's first site, window cell
@@ -1131,8 +1140,24 @@ static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cu
                       (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
     int grid = tiles < grid_cap ? tiles : grid_cap;
     if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
-    lean_sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kLeanThreads, smem, stream>>>(a, tmap);
-    return cudaGetLastError();
+    // Programmatic launch: the grid may start its prologue while the previous
+    // kernel on the stream ends (the kernel waits before it reads pass data).
+    // GLAZIER_SWEEP_PDL=0 launches it plainly.
+    static const int pdl = [] {
+        const char *env = std::getenv("GLAZIER_SWEEP_PDL");
+        return env && env[0] == '0' ? 0 : 1;
+    }();
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kLeanThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, lean_sweep_kernel<DIM, NOFF, UNIFORM>, a, tmap);
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
