@@ -714,8 +714,6 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
     }
     const int W = a.g.w, H = a.g.h, D = a.g.d;
 
-    rotate_tallies<DIM>(a);
-
     const bool small_types = a.n_types <= kSmemTypes;
     if (small_types)
         for (int i = tid; i < a.n_types * a.n_types; i += blockDim.x) S.contact[i] = a.t.contact[i];
@@ -728,6 +726,11 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.mbar[1])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // Nothing above reads what the previous pass writes; a programmatic launch
+    // may have started this grid before it ended (see launch_lean).
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    rotate_tallies<DIM>(a);
     __syncthreads();
 
     const int tiles = ((W + T::TX - 1) / T::TX) * ((H + T::TY - 1) / T::TY) * (DIM == 3 ? (D + T::TZ - 1) / T::TZ : 1);
@@ -1119,6 +1122,15 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
     }
 }
 
+// Whether sweeps launch programmatically (GLAZIER_SWEEP_PDL=0: plainly).
+static int programmatic_launch() {
+    static const int on = [] {
+        const char *env = std::getenv("GLAZIER_SWEEP_PDL");
+        return env && env[0] == '0' ? 0 : 1;
+    }();
+    return on;
+}
+
 template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cudaStream_t stream) {
     using T = Tile<DIM>;
@@ -1143,10 +1155,6 @@ static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cu
     // Programmatic launch: the grid may start its prologue while the previous
     // kernel on the stream ends (the kernel waits before it reads pass data).
     // GLAZIER_SWEEP_PDL=0 launches it plainly.
-    static const int pdl = [] {
-        const char *env = std::getenv("GLAZIER_SWEEP_PDL");
-        return env && env[0] == '0' ? 0 : 1;
-    }();
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(kLeanThreads);
@@ -1154,7 +1162,7 @@ static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cu
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = pdl;
+    attr[0].val.programmaticStreamSerializationAllowed = programmatic_launch();
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, lean_sweep_kernel<DIM, NOFF, UNIFORM>, a, tmap);
@@ -1190,8 +1198,19 @@ static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
                       (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
     int grid = tiles < grid_cap ? tiles : grid_cap;
     if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
-    sweep_kernel<DIM, NOFF, UNIFORM><<<grid, kThreads, smem, stream>>>(a, tmap);
-    return cudaGetLastError();
+    // programmatic launch as the lean kernel's, except for a motility pass,
+    // which follows its predecessor's copy list and a memset, not a kernel
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = programmatic_launch() && !a.has_motility;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, sweep_kernel<DIM, NOFF, UNIFORM>, a, tmap);
 }
 
 template <bool UNIFORM>
