@@ -572,9 +572,12 @@ __device__ __forceinline__ void load_window_plain(const SweepLaunch &a, uint32_t
     using Smem = SweepSmem<DIM>;
     const int tid = threadIdx.x;
     const int W = a.g.w, H = a.g.h, D = a.g.d;
-    // A lattice at least a window wide wraps each coordinate at most
-    // once, by a compare; a smaller one takes the remainder.
-    const bool once = W >= T::PX && H >= T::PY && (DIM == 2 || D >= T::PZ);
+    // Where every window coordinate lies within one lattice span of it (the
+    // halo reaches back no further than a span, the last tile's window no
+    // further than one span past the end) a compare wraps it; otherwise the
+    // remainder does.
+    const auto reach = [](int n, int t, int h) { return h <= n && ((n - 1) / t) * t + t + h <= 2 * n; };
+    const bool once = reach(W, T::TX, T::HX) && reach(H, T::TY, 1) && (DIM == 2 || reach(D, T::TZ, T::HZ));
     for (int i = tid; i < Smem::WIN; i += blockDim.x) {
         const int px = i % T::PX;
         const int py = (i / T::PX) % T::PY;
@@ -1339,21 +1342,27 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
         tile_origin<DIM>(t - e.tile_prefix[pos], ra.g.w, ra.g.h, x0, y0, z0);
         return maps != nullptr && tile_interior<DIM>(ra, x0, y0, z0);
     };
-    int t = blockIdx.x;
-    if (t < e.total_tiles) {
+    // Each CTA takes a contiguous run of the schedule's tiles (runs differ by
+    // at most one tile), so consecutive tiles mostly share a replica and its
+    // launch stays in shared memory.
+    const int per = e.total_tiles / (int)gridDim.x, extra = e.total_tiles % (int)gridDim.x;
+    const int first = (int)blockIdx.x * per + ((int)blockIdx.x < extra ? (int)blockIdx.x : extra);
+    const int last = first + per + ((int)blockIdx.x < extra ? 1 : 0);
+    int t = first;
+    if (t < last) {
         int pos, x0, y0, z0;
         if (locate(t, pos, x0, y0, z0)) {
             if (tid == 0) issue_window<DIM>(maps[e.order[pos]], S.win[0], &S.mbar[0], x0, y0, z0);
             pending[0] = true;
         }
     }
-    for (int it = 0; t < e.total_tiles; t += gridDim.x, ++it) {
+    for (int it = 0; t < last; ++t, ++it) {
         const int buf = it & 1;
         int pos, x0, y0, z0;
         const bool interior = locate(t, pos, x0, y0, z0);
         const int r = e.order[pos];
-        const int next = t + gridDim.x;
-        if (next < e.total_tiles) {
+        const int next = t + 1;
+        if (next < last) {
             int npos, nx0, ny0, nz0;
             if (locate(next, npos, nx0, ny0, nz0)) {
                 if (tid == 0) issue_window<DIM>(maps[e.order[npos]], S.win[buf ^ 1], &S.mbar[buf ^ 1], nx0, ny0, nz0);
@@ -1403,6 +1412,249 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS)
     }
 }
 
+// ---------------------------------------------------------------- the lean ensemble
+//
+// The lean kernel's layout over an ensemble: warp-owned target shares, the
+// window ring refilled by the last warp out, queue entries carried into the
+// warp's next tile. Warps may be on different tiles, so each ring slot holds
+// its own copy of the tile's replica launch, with the pass's fields patched
+// in; the warp that refills a slot copies the next tile's launch in first.
+// Each CTA takes a contiguous run of the schedule's tiles.
+template <int DIM>
+struct LeanEnsembleSmem {
+    LeanSmem<DIM> s;
+    SweepLaunch desc[kLeanStages];  // the slot's tile's replica launch
+    int org[kLeanStages][4];        // the slot's tile: origin x, y, z, replica
+};
+
+// The schedule's tile t: its replica's launch (pass fields patched) and
+// origin into slot `slot`, by the whole warp; lane 0 then starts its window
+// (a tensor copy, or a bare arrival when the replica's window takes plain
+// loads).
+template <int DIM>
+__device__ __forceinline__ void lean_ens_fill(const EnsembleLaunch &e, LeanEnsembleSmem<DIM> &E, int t, int slot,
+                                              long long step, long long pass) {
+    using T = Tile<DIM>;
+    const int lane = threadIdx.x & 31;
+    const int pos = replica_of_tile(e.tile_prefix, e.n, t);
+    const int r = e.order[pos];
+    const EnsembleReplica &rep = e.replicas[r];
+    const int *src = reinterpret_cast<const int *>(&rep.a);
+    int *dst = reinterpret_cast<int *>(&E.desc[slot]);
+    for (int i = lane; i < (int)(sizeof(SweepLaunch) / sizeof(int)); i += 32) dst[i] = src[i];
+    __syncwarp();
+    if (lane == 0) {
+        SweepLaunch &d = E.desc[slot];
+        d.colour = e.colour;
+        d.step = (int32_t)step;
+        d.key_pick = stream_key(rep.seed, d.step, e.colour, 0);
+        d.key_accept = stream_key(rep.seed, d.step, e.colour, 1);
+        d.vs_base = e.vs_base[pass % 2] + rep.cell_off;
+        d.vs_prev = e.vs_delta[(pass + 2) % 3] + rep.cell_off;
+        d.vs_cur = reinterpret_cast<unsigned long long *>(e.vs_delta[pass % 3] + rep.cell_off);
+        int x0, y0, z0;
+        tile_origin<DIM>(t - e.tile_prefix[pos], d.g.w, d.g.h, x0, y0, z0);
+        E.org[slot][0] = x0;
+        E.org[slot][1] = y0;
+        E.org[slot][2] = z0;
+        E.org[slot][3] = r;
+        E.s.issued[slot] += 1;
+        const CUtensorMap *maps = static_cast<const CUtensorMap *>(e.maps);
+        if (maps && lean_copies<DIM>(d))
+            issue_window<DIM>(maps[r], E.s.win[slot], &E.s.full[slot], x0, y0, z0);
+        else
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&E.s.full[slot])) : "memory");
+    }
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+__global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
+    lean_ensemble_kernel(const __grid_constant__ EnsembleLaunch e) {
+    using T = Tile<DIM>;
+    using Smem = LeanSmem<DIM>;
+    constexpr int PER_LANE = Smem::TPW / 32;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t raw = smem_addr(smem_raw);
+    LeanEnsembleSmem<DIM> &E = *reinterpret_cast<LeanEnsembleSmem<DIM> *>(smem_raw + ((128u - (raw & 127u)) & 127u));
+    Smem &S = E.s;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (smem_addr(S.win[0]) & 127u) {
+        if (tid == 0) atomicExch(e.error_flag, 3);
+        return;
+    }
+    const long long step = e.clock->step;
+    const long long pass = e.clock->pass + e.colour;
+    const int per = e.total_tiles / (int)gridDim.x, extra = e.total_tiles % (int)gridDim.x;
+    const int first = (int)blockIdx.x * per + ((int)blockIdx.x < extra ? (int)blockIdx.x : extra);
+    const int mine = per + ((int)blockIdx.x < extra ? 1 : 0);
+
+    if (tid == 0) {
+        for (int k = 0; k < kLeanStages; ++k) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.full[k])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&S.patched[k])), "r"(kLeanWarps));
+            S.done[k] = 0;
+            S.issued[k] = 0;
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+#pragma unroll
+    for (int k = 0; k < NOFF; ++k)
+        if (tid == k) S.woff[k] = window_offset<DIM, NOFF>(k);
+    __syncthreads();
+    if (warp == 0)
+        for (int i = 0; i < kLeanStages && i < mine; ++i) lean_ens_fill<DIM>(e, E, first + i, i, step, pass);
+    // the tally rotation over every replica's cells, its reads copied in ahead
+    const size_t rot_stride = (size_t)gridDim.x * blockDim.x;
+    const size_t rot_first = (size_t)blockIdx.x * blockDim.x + tid;
+    const int2 *rot_base = e.vs_base[pass % 2];
+    const long long *rot_prev = e.vs_delta[(pass + 2) % 3];
+#pragma unroll
+    for (int k = 0; k < kRotate; ++k) {
+        const size_t l = rot_first + k * rot_stride;
+        if (l < (size_t)e.total_cells) {
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(&S.rot_base[k * kLeanThreads + tid])),
+                         "l"(rot_base + l)
+                         : "memory");
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(&S.rot_prev[k * kLeanThreads + tid])),
+                         "l"(rot_prev + l)
+                         : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+
+    uint32_t *queue = S.queue[warp];
+    const unsigned below = (1u << lane) - 1u;
+    uint32_t patch_parity = 0;
+    int held = 0, held_slot = -1;
+
+    for (int i = 0; i < mine; ++i) {
+        const int slot = i % kLeanStages;
+        uint32_t *win = S.win[slot];
+        bool ok = wait_parity(&S.full[slot], (uint32_t)(i / kLeanStages) & 1u) != 0;
+        const SweepLaunch &a = E.desc[slot];
+        const int x0 = E.org[slot][0], y0 = E.org[slot][1], z0 = E.org[slot][2];
+        const int W = a.g.w, H = a.g.h, D = a.g.d;
+        const bool copies = e.maps != nullptr && lean_copies<DIM>(a);
+        const bool edge = !copies || !(x0 >= T::HX && x0 + T::TX + T::HX <= W && y0 >= 1 && y0 + T::TY + 1 <= H &&
+                                       (DIM == 2 || (z0 >= 1 && z0 + T::TZ + 1 <= D)));
+        if (edge && __all_sync(0xffffffffu, ok)) {
+            lean_patch<DIM>(a, win, x0, y0, z0, copies);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&S.patched[slot])) : "memory");
+            ok = wait_parity(&S.patched[slot], (patch_parity >> slot) & 1u) != 0;
+            patch_parity ^= 1u << slot;
+        }
+        if (!__all_sync(0xffffffffu, ok)) {
+            if (lane == 0) {
+                atomicExch(e.error_flag, 1);
+                for (int k = 0; k < kLeanStages; ++k)
+                    if (S.issued[k] > 0) wait_parity(&S.full[k], (uint32_t)(S.issued[k] - 1) & 1u);
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            return;
+        }
+
+        // light pass over this warp's share, behind the entries held over
+        const bool full = x0 + T::TX <= W && y0 + T::TY <= H && (DIM == 2 || z0 + T::TZ <= D);
+        const uint32_t tile_base = (uint32_t)((z0 * H + y0) * W + x0);
+        uint32_t entries[PER_LANE];
+        unsigned masks[PER_LANE];
+#pragma unroll
+        for (int k = 0; k < PER_LANE; ++k) {
+            const int j = warp * Smem::TPW + k * 32 + lane;
+            int lx, ly, lz;
+            target_of<DIM>(j, e.colour, lx, ly, lz);
+            const bool in = full || (x0 + lx < W && y0 + ly < H && (DIM == 2 || z0 + lz < D));
+            bool active = false;
+            int pick = 0;
+            if (in) {
+                const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
+                pick = (int)(draw(a.key_pick, tile_base + (uint32_t)((lz * H + ly) * W + lx)) % (uint64_t)NOFF);
+                active = win[wc] != win[wc + S.woff[pick]];
+            }
+            entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
+            masks[k] = __ballot_sync(0xffffffffu, active);
+        }
+        int total = held;
+#pragma unroll
+        for (int k = 0; k < PER_LANE; ++k) {
+            if (masks[k] & (1u << lane)) queue[total + __popc(masks[k] & below)] = entries[k];
+            total += __popc(masks[k]);
+        }
+        __syncwarp();
+        int taken = 0;
+        for (;;) {
+            const int n = total - taken;
+            if (n < 32 && taken >= held) break;
+            const int q = taken + lane;
+            if (q < total) {
+                const int s_ = q < held ? held_slot : slot;
+                price_and_commit<DIM, NOFF, UNIFORM, false>(E.desc[s_], S.woff, nullptr, nullptr, S.win[s_], queue[q],
+                                                            E.org[s_][0], E.org[s_][1], E.org[s_][2], false);
+            }
+            taken += n < 32 ? n : 32;
+        }
+        __syncwarp();
+        if (held_slot >= 0) {
+            // release the previous tile's slot; the last warp out refills it
+            int last_out = 0;
+            if (lane == 0) {
+                __threadfence_block();
+                last_out = atomicAdd(&S.done[held_slot], 1) == kLeanWarps - 1;
+                if (last_out) S.done[held_slot] = 0;
+            }
+            last_out = __shfl_sync(0xffffffffu, last_out, 0);
+            if (last_out && i - 1 + kLeanStages < mine) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                lean_ens_fill<DIM>(e, E, first + i - 1 + kLeanStages, held_slot, step, pass);
+            }
+        }
+        const int keep = total - taken;
+        if (taken > 0 && keep > 0) {
+            const uint32_t v = lane < keep ? queue[taken + lane] : 0u;
+            __syncwarp();
+            if (lane < keep) queue[lane] = v;
+            __syncwarp();
+        }
+        held = keep;
+        held_slot = slot;
+    }
+    if (mine > 0) {
+        if (lane < held)
+            price_and_commit<DIM, NOFF, UNIFORM, false>(E.desc[held_slot], S.woff, nullptr, nullptr, S.win[held_slot],
+                                                        queue[lane], E.org[held_slot][0], E.org[held_slot][1],
+                                                        E.org[held_slot][2], false);
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            atomicAdd(&S.done[held_slot], 1);
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    int2 *next_base = e.vs_base[(pass + 1) % 2];
+    long long *clear = e.vs_delta[(pass + 1) % 3];
+#pragma unroll
+    for (int k = 0; k < kRotate; ++k) {
+        const size_t l = rot_first + k * rot_stride;
+        if (l < (size_t)e.total_cells) {
+            int dv, ds;
+            unpack_delta(S.rot_prev[k * kLeanThreads + tid], dv, ds);
+            const int2 b = S.rot_base[k * kLeanThreads + tid];
+            next_base[l] = make_int2(b.x + dv, b.y + ds);
+            clear[l] = 0;
+        }
+    }
+    for (size_t l = rot_first + kRotate * rot_stride; l < (size_t)e.total_cells; l += rot_stride) {
+        int dv, ds;
+        unpack_delta(rot_prev[l], dv, ds);
+        const int2 b = rot_base[l];
+        next_base[l] = make_int2(b.x + dv, b.y + ds);
+        clear[l] = 0;
+    }
+}
+
 __global__ void clock_advance_kernel(EnsembleClock *clock, int ncol) {
     clock->step += 1;
     clock->pass += ncol;
@@ -1426,8 +1678,45 @@ static int ensemble_cap() {
     return cap;
 }
 
+// Whether ensembles take the lean kernel (GLAZIER_ENSEMBLE_LEAN=0: the
+// barrier-per-tile one).
+static bool lean_ensemble() {
+    static const bool on = [] {
+        const char *env = std::getenv("GLAZIER_ENSEMBLE_LEAN");
+        return !(env && env[0] == '0');
+    }();
+    return on;
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+static int lean_ensemble_cap() {
+    static int cap = 0;
+    if (!cap) {
+        const size_t smem = sizeof(LeanEnsembleSmem<DIM>) + 128;
+        if (cudaFuncSetAttribute(lean_ensemble_kernel<DIM, NOFF, UNIFORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem))
+            return 0;
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lean_ensemble_kernel<DIM, NOFF, UNIFORM>,
+                                                          kLeanThreads, smem))
+            return 0;
+        cap = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    return cap;
+}
+
 template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t ensemble_launch(const EnsembleLaunch &e, cudaStream_t stream) {
+    if (lean_ensemble()) {
+        const int cap = lean_ensemble_cap<DIM, NOFF, UNIFORM>();
+        if (!cap) return cudaErrorInvalidConfiguration;
+        int grid = e.total_tiles < cap ? e.total_tiles : cap;
+        if (e.max_ctas > 0 && grid > e.max_ctas) grid = e.max_ctas;
+        const size_t smem = sizeof(LeanEnsembleSmem<DIM>) + 128;
+        lean_ensemble_kernel<DIM, NOFF, UNIFORM><<<grid, kLeanThreads, smem, stream>>>(e);
+        return cudaGetLastError();
+    }
     const int cap = ensemble_cap<DIM, NOFF, UNIFORM>();
     if (!cap) return cudaErrorInvalidConfiguration;
     int grid = e.total_tiles < cap ? e.total_tiles : cap;
@@ -1459,12 +1748,17 @@ cudaError_t launch_clock_advance(EnsembleClock *clock, int ncol, cudaStream_t st
     return cudaGetLastError();
 }
 
+template <int DIM, int NOFF, bool UNIFORM>
+static int grid_cap_of() {
+    return lean_ensemble() ? lean_ensemble_cap<DIM, NOFF, UNIFORM>() : ensemble_cap<DIM, NOFF, UNIFORM>();
+}
+
 template <bool UNIFORM>
 static int cap_any(int dim, int n_off) {
-    if (dim == 2) return n_off == 4 ? ensemble_cap<2, 4, UNIFORM>() : ensemble_cap<2, 8, UNIFORM>();
-    if (n_off == 6) return ensemble_cap<3, 6, UNIFORM>();
-    if (n_off == 18) return ensemble_cap<3, 18, UNIFORM>();
-    return ensemble_cap<3, 26, UNIFORM>();
+    if (dim == 2) return n_off == 4 ? grid_cap_of<2, 4, UNIFORM>() : grid_cap_of<2, 8, UNIFORM>();
+    if (n_off == 6) return grid_cap_of<3, 6, UNIFORM>();
+    if (n_off == 18) return grid_cap_of<3, 18, UNIFORM>();
+    return grid_cap_of<3, 26, UNIFORM>();
 }
 
 int ensemble_grid_cap(int dim, int n_off, bool uniform) { return uniform ? cap_any<true>(dim, n_off) : cap_any<false>(dim, n_off); }
