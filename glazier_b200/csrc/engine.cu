@@ -134,7 +134,10 @@ struct glz_gpu {
     int field_cur[glz::kMaxSpecies] = {};
     uint64_t pass_no = 0, mcs = 0;
     bool use_tma = false;
-    bool lean = false;  // the sweep prices contact, volume and surface only
+    bool lean = false;    // the sweep prices contact, volume and surface only
+    bool direct = false;  // ... on a lattice small enough for the direct kernel
+    bool resident = false;  // ... with nothing between passes: every MCS in one launch
+    unsigned *barrier = nullptr;  // the resident sweep's grid barrier
     int max_ctas = 0;
     int uniform = -1;
     bool uniform_exact = false;
@@ -331,7 +334,9 @@ void find_uniform_type(glz_gpu *h, const double *contact, int n_types) {
     }
 }
 
-int sweep_pass(glz_gpu *h, int colour) {
+// The launch of the colour pass `colour` at the engine's current step and
+// pass number.
+glz::SweepLaunch pass_launch(glz_gpu *h, int colour) {
     const uint64_t p = h->pass_no;
     glz::SweepLaunch a{};
     a.g = h->g;
@@ -380,9 +385,15 @@ int sweep_pass(glz_gpu *h, int colour) {
     for (int s = 0; s < h->n_species; ++s) a.fields[s] = h->field_ptr(s, h->field_cur[s]);
     a.use_tma = h->use_tma;
     a.lean = h->lean;
+    a.direct = h->direct;
     a.max_ctas = h->max_ctas;
     a.tensor_map = h->use_tma ? &h->tmap : nullptr;
     a.error_flag = h->error_flag;
+    return a;
+}
+
+int sweep_pass(glz_gpu *h, int colour) {
+    const glz::SweepLaunch a = pass_launch(h, colour);
     CU(glz::launch_sweep(a, h->stream));
     if (h->has_motility) CU(glz::launch_apply_copies(a, h->activity, h->stream));
     h->pass_no += 1;
@@ -472,11 +483,75 @@ int check_error_flag(glz_gpu *h) {
     if (flag == 1) return fail(GLZ_DRIVER, "a sweep tile's tensor copy did not complete within its wait limit");
     if (flag == 2) return fail(GLZ_INVALID, "a label is not below the cell type count");
     if (flag == 3) return fail(GLZ_DRIVER, "the sweep's shared-memory window was not 128-byte aligned");
+    if (flag == 4) return fail(GLZ_DRIVER, "a resident sweep's grid barrier did not complete within its wait limit");
     return GLZ_OK;
 }
 
 // The step schedule, with each phase bracketed by events when `ms` is given.
+// Every MCS of the call in one cooperative launch. GLZ_OK with *done false
+// when the blocks cannot all be resident (nothing launched; the caller runs
+// the passes one by one, and later calls do too).
+int run_resident(glz_gpu *h, uint64_t steps, double *ms, bool *done) {
+    *done = false;
+    glz::ResidentLaunch r{};
+    r.a = pass_launch(h, 0);
+    r.seed = h->seed;
+    r.step0 = (int32_t)h->mcs;
+    r.mcs = (int)steps;
+    r.pass0 = (long long)h->pass_no;
+    for (int k = 0; k < 2; ++k) r.vs_base[k] = h->t.vs_base[k];
+    for (int k = 0; k < 3; ++k) r.vs_delta[k] = h->t.vs_delta[k];
+    r.barrier = h->barrier;
+    cudaEvent_t ev[2] = {};
+    if (ms) {
+        for (auto &e : ev) CU(cudaEventCreate(&e));
+        ms[0] = ms[1] = ms[2] = 0.0;
+    }
+    CU(cudaMemsetAsync(h->barrier, 0, 2 * sizeof(unsigned), h->stream));
+    if (ms) CU(cudaEventRecord(ev[0], h->stream));
+    const cudaError_t e = glz::launch_resident_sweep(r, h->stream);
+    if (e == cudaErrorCooperativeLaunchTooLarge) {
+        cudaGetLastError();
+        h->resident = false;
+        for (auto &x : ev)
+            if (x) cudaEventDestroy(x);
+        return GLZ_OK;
+    }
+    if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("resident sweep: ") + cudaGetErrorString(e));
+    if (ms) {
+        CU(cudaEventRecord(ev[1], h->stream));
+        CU(cudaEventSynchronize(ev[1]));
+        float t = 0.0f;
+        CU(cudaEventElapsedTime(&t, ev[0], ev[1]));
+        ms[0] = t;
+        for (auto &x : ev) cudaEventDestroy(x);
+    }
+    h->pass_no += steps * (uint64_t)h->g.ncol;
+    h->mcs += steps;
+    *done = true;
+    CU(cudaStreamSynchronize(h->stream));
+    return check_error_flag(h);
+}
+
 int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
+    // resident launches of at most 65536 MCS, so the barrier's arrival count
+    // (blocks x passes) stays far inside 32 bits
+    double total[3] = {0.0, 0.0, 0.0};
+    while (h->resident && steps > 0) {
+        const uint64_t chunk = steps < 65536 ? steps : 65536;
+        bool done = false;
+        double part[3];
+        if (int rc = run_resident(h, chunk, ms ? part : nullptr, &done)) return rc;
+        if (!done) break;
+        if (ms)
+            for (int k = 0; k < 3; ++k) total[k] += part[k];
+        steps -= chunk;
+    }
+    if (ms && steps == 0) {
+        for (int k = 0; k < 3; ++k) ms[k] = total[k];
+        return GLZ_OK;
+    }
+    if (steps == 0) return GLZ_OK;
     cudaEvent_t ev[6] = {};
     if (ms) {
         for (auto &e : ev) CU(cudaEventCreate(&e));
@@ -650,6 +725,17 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     const char *lean_env = std::getenv("GLAZIER_SWEEP_LEAN");
     h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !h->has_external && !h->has_motility && !has_conn &&
               !(lean_env && lean_env[0] == '0');
+    // A lean model of at most 512^2 sites takes the direct kernel, whose
+    // latency is lower when a pass is a few tiles (GLAZIER_SWEEP_DIRECT=0:
+    // never, =1: at any size).
+    const char *direct_env = std::getenv("GLAZIER_SWEEP_DIRECT");
+    const int direct_mode = direct_env ? (direct_env[0] == '0' ? 0 : 1) : -1;
+    h->direct = h->lean && (direct_mode == 1 || (direct_mode == -1 && sites <= 512LL * 512LL));
+    // With no fields, division or death there is nothing between colour
+    // passes: a direct model runs every MCS of a call in one cooperative
+    // launch (GLAZIER_SWEEP_RESIDENT=0: a launch per pass).
+    const char *resident_env = std::getenv("GLAZIER_SWEEP_RESIDENT");
+    h->resident = h->direct && ns == 0 && !h->has_pop && !(resident_env && resident_env[0] == '0');
     h->host_tv = tv;
     h->host_lv = lv;
     h->host_ts = ts;
@@ -698,6 +784,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         if (cudaMemset(h->pending_count, 0, sizeof(int))) return bail(fail(GLZ_DRIVER, "memset failed"));
     }
     if ((rc = dev_alloc(&h->error_flag, 1))) return bail(rc);
+    if ((rc = dev_alloc(&h->barrier, 2))) return bail(rc);
     if ((rc = dev_alloc(&h->medium, 2))) return bail(rc);
     if ((rc = dev_alloc(&h->counters, 2))) return bail(rc);
     if (cudaMemsetAsync(h->error_flag, 0, sizeof(int), h->stream)) return bail(fail(GLZ_DRIVER, "memset failed"));
@@ -894,7 +981,7 @@ void glz_gpu_destroy(glz_gpu *h) {
     cudaFree(h->activity); cudaFree(h->pending); cudaFree(h->pending_count); cudaFree(h->nematic); cudaFree(h->lnem);
     cudaFree(h->tl); cudaFree(h->ll); cudaFree(h->divv); cudaFree(h->death); cudaFree(h->connected);
     cudaFree(h->labels); cudaFree(h->cell_type); cudaFree(h->field_buf); cudaFree(h->dose);
-    cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->counters);
+    cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->barrier); cudaFree(h->counters);
     free_tallies(h->t);
     free_population(h);
     if (h->stream) cudaStreamDestroy(h->stream);

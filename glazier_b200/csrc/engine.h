@@ -94,12 +94,30 @@ struct SweepLaunch {
     const float *fields[kMaxSpecies];
     int use_tma;
     int lean;                // take the lean kernel: no length, chemotaxis, connectivity or moment tracking
+    int direct;              // a lean model small enough for the direct kernel (one thread per target)
     int max_ctas;            // > 0 caps the persistent grid (each CTA then walks more tiles)
     const void *tensor_map;  // CUtensorMap in device-visible memory, or null
     int *error_flag;
 };
 
 cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream);
+
+// Every requested MCS of a small lean model with nothing between its passes
+// in one cooperative launch (sweep.cu, the resident sweep).
+struct ResidentLaunch {
+    SweepLaunch a;           // static fields; the pass fields are set per pass
+    uint64_t seed;
+    int32_t step0;           // the first MCS's step number
+    int mcs;                 // MCS to run
+    long long pass0;         // the first pass's number (the tally rotation's phase)
+    int2 *vs_base[2];
+    long long *vs_delta[3];
+    unsigned *barrier;       // [0] arrivals, [1] barriers completed; zero at launch
+};
+
+// cudaErrorCooperativeLaunchTooLarge (and nothing launched) when the blocks
+// cannot all be resident at once.
+cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream);
 
 // Apply a motility pass's listed copies: the label, and the activity of a
 // type with a maximum (lib.rs:696-698); then clear the list.

@@ -1125,6 +1125,287 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
     }
 }
 
+// ---------------------------------------------------------------- the direct sweep
+//
+// Small lattices of the lean models take a kernel with no staging at all:
+// one thread per target, the labels read where they lie (a target's
+// neighbours are other colours, which no copy in the pass changes), priced
+// with price_and_commit's arithmetic operation for operation. The lean
+// kernel's window ring, patches and queues cost more latency than they save
+// when a pass is a few tiles.
+// The per-pass view of the tallies and draws a direct pass reads.
+struct PassView {
+    int colour;
+    uint64_t key_pick, key_accept;
+    const int2 *vs_base;
+    const long long *vs_prev;
+    unsigned long long *vs_cur;
+};
+
+// A global load that (CG) bypasses the SM's L1, for data other blocks wrote
+// since this kernel began: L1 is not coherent across SMs within a launch.
+template <bool CG, typename V>
+__device__ __forceinline__ V load(const V *p) {
+    if constexpr (CG)
+        return __ldcg(p);
+    else
+        return *p;
+}
+
+// The per-colour guard of keeps_other_colour, for a direct pass.
+template <bool CG>
+__device__ __noinline__ bool direct_keeps_other_colour(const SweepLaunch &a, int colour, uint32_t old) {
+    int other = 0;
+    for (int c = 0; c < a.g.ncol; ++c)
+        if (c != colour) other += load<CG>(&a.vol_by_colour[(size_t)old * a.g.ncol + c]);
+    return other != 0;
+}
+
+// Target j of a direct pass: the labels read where they lie (a target's
+// neighbours are other colours, which no copy in the pass changes), priced
+// with price_and_commit's arithmetic operation for operation.
+template <int DIM, int NOFF, bool UNIFORM, bool CG>
+__device__ __forceinline__ void direct_target(const SweepLaunch &a, const PassView &v, int j) {
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    const int hw = W / 2, hh = H / 2;
+    const int x = 2 * (j % hw) + (v.colour & 1);
+    const int y = 2 * ((j / hw) % hh) + ((v.colour >> 1) & 1);
+    const int z = DIM == 3 ? 2 * (j / (hw * hh)) + ((v.colour >> 2) & 1) : 0;
+    const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
+    const int zm = z == 0 ? D - 1 : z - 1, zp = z == D - 1 ? 0 : z + 1;
+    const auto at = [&](int k) -> uint32_t {
+        const int dx = neighbour_offset<DIM, NOFF>(k, 0), dy = neighbour_offset<DIM, NOFF>(k, 1),
+                  dz = neighbour_offset<DIM, NOFF>(k, 2);
+        const int nx = dx < 0 ? xm : (dx > 0 ? xp : x), ny = dy < 0 ? ym : (dy > 0 ? yp : y),
+                  nz = dz < 0 ? zm : (dz > 0 ? zp : z);
+        return (uint32_t)((nz * H + ny) * W + nx);
+    };
+    const uint32_t target = (uint32_t)((z * H + y) * W + x);
+    const int pick = (int)(draw(v.key_pick, target) % (uint64_t)NOFF);
+    uint32_t source = 0;
+#pragma unroll
+    for (int k = 0; k < NOFF; ++k)
+        if (k == pick) source = at(k);
+    const uint32_t old = load<CG>(&a.labels[target]), nw = load<CG>(&a.labels[source]);
+    if (old == nw) return;
+    const int2 base_old = load<CG>(&v.vs_base[old]), base_new = load<CG>(&v.vs_base[nw]);
+    const long long prev_old = load<CG>(&v.vs_prev[old]), prev_new = load<CG>(&v.vs_prev[nw]);
+    const int t_old = UNIFORM ? a.uniform_type : a.cell_type[old];
+    const int t_new = UNIFORM ? a.uniform_type : a.cell_type[nw];
+    float delta = 0.0f;
+    int like_old = 0, like_new = 0;
+    if (UNIFORM) {
+#pragma unroll
+        for (int k = 0; k < NOFF; ++k) {
+            const uint32_t ln = load<CG>(&a.labels[at(k)]);
+            like_old += ln == old;
+            like_new += ln == nw;
+        }
+        delta = __fmul_rn(a.uniform_contact, (float)(like_old - like_new));
+    } else {
+#pragma unroll
+        for (int k = 0; k < NOFF; ++k) {
+            const uint32_t ln = load<CG>(&a.labels[at(k)]);
+            const int tn = ln == old ? t_old : (ln == nw ? t_new : (int)a.cell_type[ln]);
+            if (ln != old)
+                delta = __fsub_rn(delta, a.t.contact[t_old * a.n_types + tn]);
+            else
+                ++like_old;
+            if (ln != nw)
+                delta = __fadd_rn(delta, a.t.contact[t_new * a.n_types + tn]);
+            else
+                ++like_new;
+        }
+    }
+    if (old != 0 && like_old == 0 && !direct_keeps_other_colour<CG>(a, v.colour, old)) return;
+    const int ds_old = 2 * like_old - NOFF;
+    const int ds_new = NOFF - 2 * like_new;
+    int dv, ds;
+    unpack_delta(prev_old, dv, ds);
+    const int vol_old = base_old.x + dv, surf_old = base_old.y + ds;
+    unpack_delta(prev_new, dv, ds);
+    const int vol_new = base_new.x + dv, surf_new = base_new.y + ds;
+    if (old != 0) {
+        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_old];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)vol_old, UNIFORM ? a.u_target_volume : a.t.target_volume[t_old]);
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, e))));
+        }
+    }
+    if (nw != 0) {
+        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_new];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)vol_new, UNIFORM ? a.u_target_volume : a.t.target_volume[t_new]);
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fadd_rn(__fmul_rn(2.0f, e), 1.0f)));
+        }
+    }
+    if (old != 0) {
+        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_old];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)surf_old, UNIFORM ? a.u_target_surface : a.t.target_surface[t_old]);
+            const float d = (float)ds_old;
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(d, __fadd_rn(__fmul_rn(2.0f, e), d))));
+        }
+    }
+    if (nw != 0) {
+        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_new];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)surf_new, UNIFORM ? a.u_target_surface : a.t.target_surface[t_new]);
+            const float d = (float)ds_new;
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(d, __fadd_rn(__fmul_rn(2.0f, e), d))));
+        }
+    }
+    const float u = to_f32(draw(v.key_accept, target));
+    if (!(delta <= 0.0f || u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
+    a.labels[target] = nw;
+    if (old != 0) {
+        atomicAdd(&v.vs_cur[old], pack_delta(-1, ds_old));
+        atomicSub(&a.vol_by_colour[(size_t)old * a.g.ncol + v.colour], 1);
+    }
+    if (nw != 0) {
+        atomicAdd(&v.vs_cur[nw], pack_delta(1, ds_new));
+        atomicAdd(&a.vol_by_colour[(size_t)nw * a.g.ncol + v.colour], 1);
+    }
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+__global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant__ SweepLaunch a) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int targets = (a.g.w / 2) * (a.g.h / 2) * (DIM == 3 ? a.g.d / 2 : 1);
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < targets) {
+        const PassView v{a.colour, a.key_pick, a.key_accept, a.vs_base, a.vs_prev, a.vs_cur};
+        direct_target<DIM, NOFF, UNIFORM, false>(a, v, j);
+    }
+    rotate_tallies<DIM>(a);
+}
+
+// ---------------------------------------------------------------- the resident sweep
+//
+// A small lean model with nothing between its colour passes but the passes
+// (no fields, division, death or infection) runs every requested MCS in one
+// cooperative launch: the direct pass's work per target, the tally rotation,
+// then a grid barrier, pass after pass. Each pass's draws and tally slots
+// follow from its number as the host would set them. Reads of what other
+// blocks wrote in earlier passes go to L2. The barrier's wait is bounded: a
+// block that gives up sets error flag 4 and returns, and the others then
+// give up at their next barrier.
+
+constexpr long long kBarrierLimit = 1LL << 25;
+
+// Barrier number k of the launch (k = 0, 1, ...): false if it timed out.
+__device__ __forceinline__ bool resident_barrier(unsigned *bar, unsigned k) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) + 1u == gridDim.x * (k + 1u)) {
+            __threadfence();
+            atomicExch(&bar[1], k + 1u);
+        } else {
+            long long spin = 0;
+            while (atomicAdd(&bar[1], 0u) < k + 1u) {
+                if (++spin > kBarrierLimit) {
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+__global__ void __launch_bounds__(256) resident_sweep_kernel(const __grid_constant__ ResidentLaunch r) {
+    const SweepLaunch &a = r.a;
+    const int targets = (a.g.w / 2) * (a.g.h / 2) * (DIM == 3 ? a.g.d / 2 : 1);
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    unsigned k = 0;
+    for (int m = 0; m < r.mcs; ++m) {
+        const int32_t step = (int32_t)((uint32_t)r.step0 + (uint32_t)m);
+        for (int c = 0; c < a.g.ncol; ++c) {
+            const long long p = r.pass0 + (long long)m * a.g.ncol + c;
+            const PassView v{c, stream_key(r.seed, step, c, 0), stream_key(r.seed, step, c, 1), r.vs_base[p % 2],
+                             r.vs_delta[(p + 2) % 3], reinterpret_cast<unsigned long long *>(r.vs_delta[p % 3])};
+            if (j < targets) direct_target<DIM, NOFF, UNIFORM, true>(a, v, j);
+            // the rotation for the next pass, which no thread of this one reads
+            int2 *next_base = r.vs_base[(p + 1) % 2];
+            long long *clear = r.vs_delta[(p + 1) % 3];
+            for (size_t l = j; l < (size_t)a.n_labels; l += stride) {
+                int dv, ds;
+                unpack_delta(__ldcg(&v.vs_prev[l]), dv, ds);
+                const int2 b = __ldcg(&v.vs_base[l]);
+                next_base[l] = make_int2(b.x + dv, b.y + ds);
+                clear[l] = 0;
+            }
+            if (!resident_barrier(r.barrier, k++)) {
+                if (threadIdx.x == 0) atomicExch(a.error_flag, 4);
+                return;
+            }
+        }
+    }
+}
+
+// Run `mcs` MCS of a small lean model in one cooperative launch, or return
+// cudaErrorCooperativeLaunchTooLarge (nothing launched) when its blocks
+// cannot all be resident.
+template <int DIM, int NOFF, bool UNIFORM>
+static cudaError_t launch_resident(const ResidentLaunch &r, cudaStream_t stream) {
+    const int targets = (r.a.g.w / 2) * (r.a.g.h / 2) * (DIM == 3 ? r.a.g.d / 2 : 1);
+    const int blocks = (targets + 255) / 256;
+    static int most = 0;
+    if (!most) {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaError_t e = cudaGetDevice(&dev)) return e;
+        if (cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return e;
+        if (cudaError_t e =
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resident_sweep_kernel<DIM, NOFF, UNIFORM>, 256, 0))
+            return e;
+        most = sms * per_sm;
+    }
+    if (blocks > most) return cudaErrorCooperativeLaunchTooLarge;
+    void *args[] = {const_cast<ResidentLaunch *>(&r)};
+    return cudaLaunchCooperativeKernel((const void *)resident_sweep_kernel<DIM, NOFF, UNIFORM>, dim3(blocks), dim3(256),
+                                       args, 0, stream);
+}
+
+template <bool UNIFORM>
+static cudaError_t resident_any(const ResidentLaunch &r, cudaStream_t stream) {
+    if (r.a.g.dim == 2) {
+        if (r.a.g.n_off == 4) return launch_resident<2, 4, UNIFORM>(r, stream);
+        if (r.a.g.n_off == 8) return launch_resident<2, 8, UNIFORM>(r, stream);
+    } else {
+        if (r.a.g.n_off == 6) return launch_resident<3, 6, UNIFORM>(r, stream);
+        if (r.a.g.n_off == 18) return launch_resident<3, 18, UNIFORM>(r, stream);
+        if (r.a.g.n_off == 26) return launch_resident<3, 26, UNIFORM>(r, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream) {
+    for (int k = 0; k < r.a.g.n_off; ++k)
+        for (int axis = 0; axis < 3; ++axis) {
+            const int want = r.a.g.dim == 2 ? (r.a.g.n_off == 4 ? neighbour_offset<2, 4>(k, axis)
+                                                                 : neighbour_offset<2, 8>(k, axis))
+                                            : (r.a.g.n_off == 6    ? neighbour_offset<3, 6>(k, axis)
+                                               : r.a.g.n_off == 18 ? neighbour_offset<3, 18>(k, axis)
+                                                                   : neighbour_offset<3, 26>(k, axis));
+            if (r.a.g.off[k][axis] != want) return cudaErrorInvalidValue;
+        }
+    return r.a.uniform_type >= 0 && r.a.uniform_contact_exact ? resident_any<true>(r, stream)
+                                                              : resident_any<false>(r, stream);
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream);
+
 // Whether sweeps launch programmatically (GLAZIER_SWEEP_PDL=0: plainly).
 static int programmatic_launch() {
     static const int on = [] {
@@ -1132,6 +1413,21 @@ static int programmatic_launch() {
         return env && env[0] == '0' ? 0 : 1;
     }();
     return on;
+}
+
+template <int DIM, int NOFF, bool UNIFORM>
+static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
+    const int targets = (a.g.w / 2) * (a.g.h / 2) * (DIM == 3 ? a.g.d / 2 : 1);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)((targets + 255) / 256));
+    cfg.blockDim = dim3(256);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = programmatic_launch();
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM>, a);
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
@@ -1182,7 +1478,8 @@ static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
         tmap = *static_cast<const CUtensorMap *>(a.tensor_map);
     else
         memset(&tmap, 0, sizeof tmap);
-    if (a.lean) return launch_lean<DIM, NOFF, UNIFORM>(a, tmap, stream);
+    if (a.lean) return a.direct ? launch_direct<DIM, NOFF, UNIFORM>(a, stream)
+                                : launch_lean<DIM, NOFF, UNIFORM>(a, tmap, stream);
     using T = Tile<DIM>;
     static int grid_cap = 0;
     const size_t smem = sizeof(SweepSmem<DIM>) + 128;

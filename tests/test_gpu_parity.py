@@ -173,19 +173,25 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("lean", ["1", "0"])
+@pytest.mark.parametrize("kernel", ["resident", "direct", "lean", "general"])
 @pytest.mark.parametrize("ctas", ["0", "3"])
 @pytest.mark.parametrize("tma", ["1", "0"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, lean, monkeypatch):
+def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, kernel, monkeypatch):
     """`ctas` 3 caps the sweep's persistent grid at three CTAs, so every CTA
-    walks several tiles and every window buffer takes tensor copies; `lean` 0
-    keeps the model on the general kernel."""
+    walks several tiles and every window buffer takes tensor copies; `kernel`
+    forces the lean models onto the resident (every MCS of a call in one
+    launch, for models with nothing between passes), the direct, the lean or
+    the general kernel (models with other terms always take the general one)."""
+    if kernel in ("resident", "direct") and (tma == "0" or ctas == "3"):
+        pytest.skip("the resident and direct kernels stage nothing and have no persistent grid")
     made, steps = CASES[name]()
     start, fields = made if isinstance(made, tuple) else (made, None)
     monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
     monkeypatch.setenv("GLAZIER_SWEEP_CTAS", ctas)
-    monkeypatch.setenv("GLAZIER_SWEEP_LEAN", lean)
+    monkeypatch.setenv("GLAZIER_SWEEP_LEAN", "0" if kernel == "general" else "1")
+    monkeypatch.setenv("GLAZIER_SWEEP_DIRECT", "1" if kernel in ("resident", "direct") else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_RESIDENT", "1" if kernel == "resident" else "0")
     gpu = device.GpuSimulation.from_start(start, fields)
     replay = ReplayOracle.from_start(start, fields)
     for chunk in (1, steps - 1):
