@@ -325,6 +325,58 @@ def published_rows(device: int) -> dict:
     return rows
 
 
+def coupling_leg(device: int, rounds: int = 3, steps: int = 250) -> dict:
+    """The reference's coupling round (README.md:332-337): a 512^2 monolayer
+    of 8 x 8 cells under a nematic field (contact [0,16,16,8], lambda_V 2,
+    V_t 64, lambda_nematic 6, T 10, Moore, seed 1), rounds of 250 MCS, after
+    each the lattice out and a new field in. Timed on the host clock per
+    round: the steps, and the hand-over both ways, through host copies
+    (``labels`` + ``set_nematic_field``) and through device tensors
+    (``labels_tensor`` + ``set_nematic_field_tensor``). The new field is a
+    function of the labels computed where the lattice is (numpy or torch);
+    the reference's figures: 0.21 s of steps and 0.08 s of transfer a round."""
+    import math
+
+    import numpy as np
+    import torch
+
+    from glazier_b200.blueprint import CellType, Model, Start
+    from glazier_b200.engine import GpuSimulation
+
+    m = Model(width=512, height=512, contact=[0.0, 16.0, 16.0, 8.0],
+              types=[CellType(), CellType(target_volume=64.0, lambda_volume=2.0, lambda_nematic=6.0)],
+              temperature=10.0, neighbour_order=2, seed=1)
+    m.nematic = np.tile([math.cos(1.2), math.sin(1.2)], (512 * 512, 1))
+    out = {"lattice": "512^2", "mcs_per_round": steps, "rounds": rounds, "published_steps_s": 0.21,
+           "published_transfer_s": 0.08}
+    def hand_over(sim, mode):
+        if mode == "host":
+            lab = sim.labels().astype(np.int64)
+            q = np.stack([((lab % 7) - 3) / 4.0, ((lab % 5) - 2) / 4.0], axis=1)
+            sim.set_nematic_field(q)
+        else:
+            lab = sim.labels_tensor().reshape(-1)
+            q = torch.stack([((lab % 7) - 3).float() / 4, ((lab % 5) - 2).float() / 4], dim=1)
+            sim.set_nematic_field_tensor(q)
+        torch.cuda.synchronize()
+
+    for mode in ("host", "device"):
+        sim = GpuSimulation.from_start(Start.tiled(m, 8), device=device)
+        sim.step(2)
+        hand_over(sim, mode)  # one-time costs (torch's kernels load on first use)
+        step_s = hand_s = 0.0
+        for _ in range(rounds):
+            t = time.perf_counter()
+            sim.step(steps)
+            step_s += time.perf_counter() - t
+            t = time.perf_counter()
+            hand_over(sim, mode)
+            hand_s += time.perf_counter() - t
+        sim.close()
+        out[mode] = {"steps_s_per_round": step_s / rounds, "handover_s_per_round": hand_s / rounds}
+    return out
+
+
 def volume_leg(mcs: int, device: int, peak: float) -> dict:
     """The scaling configuration's volume: a periodic 128^3 lattice of 4096
     cubic cells of side 8, 26 neighbours, J 10, lambda_V 1 at V_t 512,
@@ -530,6 +582,7 @@ def run_ours(args) -> None:
     if world == 1 and not args.no_published:
         line["volume"] = volume_leg(20, torch.cuda.current_device(), peak)
         line["published_rows"] = published_rows(torch.cuda.current_device())
+        line["coupling"] = coupling_leg(torch.cuda.current_device())
     if world == 1 and not args.no_infection:
         line["infection"] = infection_compare(200, 20, torch.cuda.current_device())
     if world == 1 and not args.no_adjoint:

@@ -136,6 +136,10 @@ def lib():
     L.glz_set_device.argtypes = [C.c_int]
     L.glz_gpu_set_labels.restype = C.c_int
     L.glz_gpu_set_labels.argtypes = [_P, _P, C.c_size_t]
+    L.glz_gpu_set_labels_device.restype = C.c_int
+    L.glz_gpu_set_labels_device.argtypes = [_P, _P, C.c_size_t]
+    L.glz_gpu_set_nematic_field_device.restype = C.c_int
+    L.glz_gpu_set_nematic_field_device.argtypes = [_P, _P, C.c_size_t]
     L.glz_gpu_step_profiled.restype = C.c_int
     L.glz_gpu_step_profiled.argtypes = [_P, C.c_uint64, C.POINTER(C.c_double)]
     L.glz_field_step_noalloc.restype = C.c_int

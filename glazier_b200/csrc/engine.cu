@@ -845,6 +845,26 @@ int glz_gpu_set_labels(glz_gpu *h, const uint32_t *labels, size_t sites) {
     return recount(h);
 }
 
+// Whether `p` is device memory of the handle's device (plain or managed).
+static bool on_device(const glz_gpu *h, const void *p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == h->device;
+}
+
+int glz_gpu_set_labels_device(glz_gpu *h, const uint32_t *labels, size_t sites) {
+    if (!h || !labels) return fail(GLZ_INVALID, "null handle or labels");
+    if (sites != (size_t)h->g.sites) return fail(GLZ_INVALID, "the lattice is not one label per site");
+    if (!on_device(h, labels)) return fail(GLZ_INVALID, "the labels are not device memory of the engine's device");
+    CU(cudaMemcpyAsync(h->labels, labels, sites * sizeof(uint32_t), cudaMemcpyDeviceToDevice, h->stream));
+    if (int rc = recount(h)) return rc;
+    CU(cudaStreamSynchronize(h->stream));
+    return GLZ_OK;
+}
+
 int glz_gpu_labels(glz_gpu *h, uint32_t *out, size_t sites) {
     if (!h || !out) return fail(GLZ_INVALID, "null handle or buffer");
     if (sites != (size_t)h->g.sites) return fail(GLZ_INVALID, "the buffer is not one label per site");
@@ -948,6 +968,23 @@ int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len) {
     for (size_t i = 0; i < len; ++i) q[i] = (float)field[i];
     CU(cudaMemcpyAsync(h->nematic, q.data(), len * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     // the per-cell sums follow the new field: settle, then recount every tally
+    if (int rc = settle(h)) return rc;
+    if (int rc = recount(h)) return rc;
+    CU(cudaStreamSynchronize(h->stream));
+    return GLZ_OK;
+}
+
+int glz_gpu_set_nematic_field_device(glz_gpu *h, const float *field, size_t len) {
+    if (!h) return fail(GLZ_INVALID, "null handle");
+    if (len != 2 * (size_t)h->g.sites) {
+        char msg[128];
+        std::snprintf(msg, sizeof msg, "nematic field has %zu sites, the lattice %d", len / 2, h->g.sites);
+        return fail(GLZ_INVALID, msg);
+    }
+    if (!h->has_nematic) return fail(GLZ_DRIVER, "the model has no nematic coupling to update");
+    if (!field) return fail(GLZ_INVALID, "null field");
+    if (!on_device(h, field)) return fail(GLZ_INVALID, "the field is not device memory of the engine's device");
+    CU(cudaMemcpyAsync(h->nematic, field, len * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
     if (int rc = settle(h)) return rc;
     if (int rc = recount(h)) return rc;
     CU(cudaStreamSynchronize(h->stream));

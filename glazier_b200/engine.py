@@ -33,6 +33,39 @@ def check(rc: int) -> None:
         raise GpuError(rc, _lib.last_error())
 
 
+class _DeviceArray:
+    """A bare ``__cuda_array_interface__`` over device memory the engine owns,
+    for ``torch.as_tensor`` to wrap without a copy (on the memory's own
+    device). Every call that writes it has synchronized its stream before
+    returning, so readers need no stream to wait on."""
+
+    def __init__(self, address: int, shape: tuple, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(address), False),
+                                         "version": 3, "strides": None, "stream": None}
+
+
+def _view(address: int, shape: tuple, typestr: str, owner):
+    import torch
+
+    t = torch.as_tensor(_DeviceArray(address, shape, typestr))
+    t._glazier_owner = owner  # the engine outlives the view while the view is referenced
+    return t
+
+
+def _device_input(tensor, dtypes: tuple, count: int, what: str):
+    """A contiguous device tensor of `count` elements of one of `dtypes`, with
+    the engine's stream ordered after the work that produced it."""
+    import torch
+
+    if not isinstance(tensor, torch.Tensor) or not tensor.is_cuda:
+        raise GpuError(GLZ_INVALID, f"the {what} is not a CUDA tensor")
+    if tensor.dtype not in dtypes:
+        raise GpuError(GLZ_INVALID, f"the {what} is {tensor.dtype}, not one of {dtypes}")
+    if tensor.numel() != count:
+        raise GpuError(GLZ_INVALID, f"the {what} has {tensor.numel()} values, not {count}")
+    return tensor.contiguous()
+
+
 class GpuSimulation:
     """One run on the device.
 
@@ -166,6 +199,50 @@ class GpuSimulation:
     def stream(self) -> int:
         """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         return int(_lib.lib().glz_gpu_stream(self._h) or 0)
+
+    def _after_torch(self, tensor) -> None:
+        """Make the engine's stream wait for torch's current stream on the
+        tensor's device, so the engine reads what torch wrote."""
+        import torch
+
+        torch.cuda.ExternalStream(self.stream, device=tensor.device).wait_stream(
+            torch.cuda.current_stream(tensor.device))
+
+    def labels_tensor(self):
+        """The lattice as a torch tensor on the device, without a copy: int32
+        per site (every label is below 2^31), shaped ``shape`` (depth,
+        height, width). It aliases the engine's own buffer: it shows what the
+        last ``step`` or restart left, stays valid until ``close``, and is for
+        reading; a changed lattice goes back through ``set_labels_tensor``.
+        The zero-copy form of ``GpuSession.labels``
+        (glazier-py/src/lib.rs:215-219)."""
+        return _view(self.device_labels(), self.shape, "<i4", self)
+
+    def field_tensor(self, index: int):
+        """Species ``index`` as a float32 torch tensor aliasing the device
+        field (the engine computes fields in f32; ``field`` widens the same
+        values to f64), shaped ``shape``; valid until the next ``step``, which
+        moves the field to its other buffer."""
+        return _view(self.device_field(index), self.shape, "<f4", self)
+
+    def set_labels_tensor(self, labels) -> None:
+        """``set_labels`` from a CUDA tensor of int32 or uint32 labels, one per
+        site (x fastest), on the engine's device: copied on the device, then
+        every tally recounted."""
+        import torch
+
+        t = _device_input(labels, (torch.int32, torch.uint32), self.sites, "lattice")
+        self._after_torch(t)
+        check(_lib.lib().glz_gpu_set_labels_device(self._h, C.c_void_p(t.data_ptr()), t.numel()))
+
+    def set_nematic_field_tensor(self, field) -> None:
+        """``set_nematic_field`` from a CUDA float32 tensor of (Q_xx, Q_xy)
+        per site, ``2 * sites`` values, on the engine's device."""
+        import torch
+
+        t = _device_input(field, (torch.float32,), 2 * self.sites, "nematic field")
+        self._after_torch(t)
+        check(_lib.lib().glz_gpu_set_nematic_field_device(self._h, C.c_void_p(t.data_ptr()), t.numel()))
 
     def device_labels(self) -> int:
         p = C.c_void_p()

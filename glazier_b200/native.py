@@ -87,6 +87,17 @@ class GpuSession:
             raise ValueError(f"expected {2 * self._sites} numbers, got {len(flat)}")
         self._sim.set_nematic_field(flat)
 
+    def labels_tensor(self):
+        """The lattice as a device tensor without a copy (int32, shaped
+        (depth, height, width)): the zero-copy ``labels`` for a solver that
+        runs on the same GPU. Valid until the session is dropped; read only."""
+        return self._sim.labels_tensor()
+
+    def set_nematic_field_tensor(self, field) -> None:
+        """``set_nematic_field`` from a CUDA float32 tensor of ``2 * sites``
+        values, (Q_xx, Q_xy) per site, without a trip through the host."""
+        self._sim.set_nematic_field_tensor(field)
+
     @property
     def mcs(self) -> int:
         """Monte Carlo steps completed."""

@@ -99,6 +99,14 @@ int glz_gpu_step(glz_gpu *h, uint64_t steps);
  * one not below the label count fails the next glz_gpu_step. */
 int glz_gpu_set_labels(glz_gpu *h, const uint32_t *labels, size_t sites);
 
+/* glz_gpu_set_labels from device memory of the handle's device (uint32 per
+ * site): the zero-copy restart for a solver that keeps the lattice on the
+ * device. The caller's writes to `labels` must be complete before the call
+ * (its stream synchronized, or the handle's stream made to wait on it); the
+ * copy and the recount run on the handle's stream and are done when the call
+ * returns. Memory of another device or of the host: GLZ_INVALID. */
+int glz_gpu_set_labels_device(glz_gpu *h, const uint32_t *labels, size_t sites);
+
 /* Run `steps` Monte Carlo steps like glz_gpu_step and report the device time
  * of each phase in milliseconds: ms[0] the colour sweeps, ms[1] the field
  * step, ms[2] division and death. No reference counterpart. */
@@ -140,6 +148,12 @@ int glz_gpu_set_infection(glz_gpu *h, int species, int from_type, int to_type, d
  * wrong length is GLZ_INVALID; a model without a nematic coupling is refused
  * with the reference's message (GLZ_DRIVER, as the reference's Driver). */
 int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len);
+
+/* glz_gpu_set_nematic_field from device memory: 2 f32 per site (q_xx, q_xy),
+ * with the same checks, recount and ordering rule as
+ * glz_gpu_set_labels_device. The host form rounds its f64 values to f32, so
+ * equal f32 values make the same run. */
+int glz_gpu_set_nematic_field_device(glz_gpu *h, const float *field, size_t len);
 
 /* Monte Carlo steps completed: `pub mcs` (lib.rs:805). */
 uint64_t glz_gpu_mcs(const glz_gpu *h);
