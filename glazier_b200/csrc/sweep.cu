@@ -1293,7 +1293,8 @@ __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant
 // block that gives up sets error flag 4 and returns, and the others then
 // give up at their next barrier.
 
-constexpr long long kBarrierLimit = 1LL << 25;
+// polls of the barrier word (each an L2 round trip, so the limit is seconds)
+constexpr long long kBarrierLimit = 1LL << 22;
 
 // Barrier number k of the launch (k = 0, 1, ...): false if it timed out.
 __device__ __forceinline__ bool resident_barrier(unsigned *bar, unsigned k) {
@@ -1307,12 +1308,13 @@ __device__ __forceinline__ bool resident_barrier(unsigned *bar, unsigned k) {
             atomicExch(&bar[1], k + 1u);
         } else {
             long long spin = 0;
-            while (atomicAdd(&bar[1], 0u) < k + 1u) {
-                if (++spin > kBarrierLimit) {
-                    ok = 0;
+            for (;;) {
+                unsigned g;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(&bar[1]) : "memory");
+                if (g >= k + 1u || ++spin > kBarrierLimit) {
+                    ok = g >= k + 1u;
                     break;
                 }
-                __nanosleep(64);
             }
         }
         __threadfence();
