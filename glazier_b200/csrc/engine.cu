@@ -137,6 +137,7 @@ struct glz_gpu {
     bool lean = false;    // the sweep prices contact, volume and surface only
     bool direct = false;  // ... on a lattice small enough for the direct kernel
     bool resident = false;  // ... with nothing between passes: every MCS in one launch
+    bool cluster = false;   // ... a plane, in one thread-block cluster's shared memory
     unsigned *barrier = nullptr;  // the resident sweep's grid barrier
     int max_ctas = 0;
     int uniform = -1;
@@ -509,7 +510,15 @@ int run_resident(glz_gpu *h, uint64_t steps, double *ms, bool *done) {
     }
     CU(cudaMemsetAsync(h->barrier, 0, 2 * sizeof(unsigned), h->stream));
     if (ms) CU(cudaEventRecord(ev[0], h->stream));
-    const cudaError_t e = glz::launch_resident_sweep(r, h->stream);
+    cudaError_t e = cudaErrorNotSupported;
+    if (h->cluster) {
+        e = glz::launch_cluster_sweep(r, h->stream);
+        if (e == cudaErrorNotSupported) {
+            cudaGetLastError();
+            h->cluster = false;  // and later calls: the plane does not fit a cluster
+        }
+    }
+    if (!h->cluster) e = glz::launch_resident_sweep(r, h->stream);
     if (e == cudaErrorCooperativeLaunchTooLarge) {
         cudaGetLastError();
         h->resident = false;
@@ -736,6 +745,10 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     // launch (GLAZIER_SWEEP_RESIDENT=0: a launch per pass).
     const char *resident_env = std::getenv("GLAZIER_SWEEP_RESIDENT");
     h->resident = h->direct && ns == 0 && !h->has_pop && !(resident_env && resident_env[0] == '0');
+    // A resident plane runs in one thread-block cluster when it fits one
+    // (GLAZIER_SWEEP_CLUSTER=0: the cooperative grid instead).
+    const char *cluster_env = std::getenv("GLAZIER_SWEEP_CLUSTER");
+    h->cluster = h->resident && g.dim == 2 && !(cluster_env && cluster_env[0] == '0');
     h->host_tv = tv;
     h->host_lv = lv;
     h->host_ts = ts;

@@ -118,6 +118,9 @@ struct ResidentLaunch {
 // cudaErrorCooperativeLaunchTooLarge (and nothing launched) when the blocks
 // cannot all be resident at once.
 cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream);
+// The same MCS in one thread-block cluster holding a small plane in shared
+// memory; cudaErrorNotSupported (nothing launched) when it does not fit one.
+cudaError_t launch_cluster_sweep(const ResidentLaunch &r, cudaStream_t stream);
 
 // Apply a motility pass's listed copies: the label, and the activity of a
 // type with a maximum (lib.rs:696-698); then clear the list.

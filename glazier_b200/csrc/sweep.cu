@@ -24,6 +24,7 @@
 // atomics whose order does not matter; a pass is therefore deterministic and
 // a host replay of the same schedule reproduces it bit for bit.
 
+#include <cooperative_groups.h>
 #include <cuda.h>
 
 #include <cstdlib>
@@ -1161,16 +1162,44 @@ __device__ __noinline__ bool direct_keeps_other_colour(const SweepLaunch &a, int
     return other != 0;
 }
 
-// Target j of a direct pass: the labels read where they lie (a target's
-// neighbours are other colours, which no copy in the pass changes), priced
-// with price_and_commit's arithmetic operation for operation.
-template <int DIM, int NOFF, bool UNIFORM, bool CG>
-__device__ __forceinline__ void direct_target(const SweepLaunch &a, const PassView &v, int j) {
+// Where a direct pass finds and puts labels and tallies: global memory, read
+// through L2 when CG (the resident kernel reads what other blocks wrote).
+template <bool CG>
+struct GlobalPass {
+    const SweepLaunch &a;
+    const PassView &v;
+    __device__ __forceinline__ uint32_t label(int x, int y, int z) const {
+        return load<CG>(&a.labels[(z * a.g.h + y) * a.g.w + x]);
+    }
+    __device__ __forceinline__ int2 base(uint32_t l) const { return load<CG>(&v.vs_base[l]); }
+    __device__ __forceinline__ long long prev(uint32_t l) const { return load<CG>(&v.vs_prev[l]); }
+    __device__ __forceinline__ bool keeps_other_colour(uint32_t old) const {
+        return direct_keeps_other_colour<CG>(a, v.colour, old);
+    }
+    __device__ __forceinline__ void put(uint32_t target, int, int, int, uint32_t nw) const { a.labels[target] = nw; }
+    __device__ __forceinline__ void tally(uint32_t l, int dv, int ds) const {
+        atomicAdd(&v.vs_cur[l], pack_delta(dv, ds));
+        atomicAdd(&a.vol_by_colour[(size_t)l * a.g.ncol + v.colour], dv);
+    }
+};
+
+// Site (x, y, z) of target j of colour `colour` in a direct pass.
+template <int DIM>
+__device__ __forceinline__ void direct_site(const SweepLaunch &a, int colour, int j, int &x, int &y, int &z) {
+    const int hw = a.g.w / 2, hh = a.g.h / 2;
+    x = 2 * (j % hw) + (colour & 1);
+    y = 2 * ((j / hw) % hh) + ((colour >> 1) & 1);
+    z = DIM == 3 ? 2 * (j / (hw * hh)) + ((colour >> 2) & 1) : 0;
+}
+
+// The copy attempt at target (x, y, z) of a direct pass, its labels and
+// tallies found through `acc`: a target's neighbours are other colours, which
+// no copy in the pass changes. Priced with price_and_commit's arithmetic
+// operation for operation.
+template <int DIM, int NOFF, bool UNIFORM, class Access>
+__device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access &acc, uint64_t key_pick,
+                                              uint64_t key_accept, int x, int y, int z) {
     const int W = a.g.w, H = a.g.h, D = a.g.d;
-    const int hw = W / 2, hh = H / 2;
-    const int x = 2 * (j % hw) + (v.colour & 1);
-    const int y = 2 * ((j / hw) % hh) + ((v.colour >> 1) & 1);
-    const int z = DIM == 3 ? 2 * (j / (hw * hh)) + ((v.colour >> 2) & 1) : 0;
     const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
     const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
     const int zm = z == 0 ? D - 1 : z - 1, zp = z == D - 1 ? 0 : z + 1;
@@ -1179,18 +1208,18 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const PassVi
                   dz = neighbour_offset<DIM, NOFF>(k, 2);
         const int nx = dx < 0 ? xm : (dx > 0 ? xp : x), ny = dy < 0 ? ym : (dy > 0 ? yp : y),
                   nz = dz < 0 ? zm : (dz > 0 ? zp : z);
-        return (uint32_t)((nz * H + ny) * W + nx);
+        return acc.label(nx, ny, nz);
     };
     const uint32_t target = (uint32_t)((z * H + y) * W + x);
-    const int pick = (int)(draw(v.key_pick, target) % (uint64_t)NOFF);
-    uint32_t source = 0;
+    const int pick = (int)(draw(key_pick, target) % (uint64_t)NOFF);
+    uint32_t nw = 0;
 #pragma unroll
     for (int k = 0; k < NOFF; ++k)
-        if (k == pick) source = at(k);
-    const uint32_t old = load<CG>(&a.labels[target]), nw = load<CG>(&a.labels[source]);
+        if (k == pick) nw = at(k);
+    const uint32_t old = acc.label(x, y, z);
     if (old == nw) return;
-    const int2 base_old = load<CG>(&v.vs_base[old]), base_new = load<CG>(&v.vs_base[nw]);
-    const long long prev_old = load<CG>(&v.vs_prev[old]), prev_new = load<CG>(&v.vs_prev[nw]);
+    const int2 base_old = acc.base(old), base_new = acc.base(nw);
+    const long long prev_old = acc.prev(old), prev_new = acc.prev(nw);
     const int t_old = UNIFORM ? a.uniform_type : a.cell_type[old];
     const int t_new = UNIFORM ? a.uniform_type : a.cell_type[nw];
     float delta = 0.0f;
@@ -1198,7 +1227,7 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const PassVi
     if (UNIFORM) {
 #pragma unroll
         for (int k = 0; k < NOFF; ++k) {
-            const uint32_t ln = load<CG>(&a.labels[at(k)]);
+            const uint32_t ln = at(k);
             like_old += ln == old;
             like_new += ln == nw;
         }
@@ -1206,7 +1235,7 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const PassVi
     } else {
 #pragma unroll
         for (int k = 0; k < NOFF; ++k) {
-            const uint32_t ln = load<CG>(&a.labels[at(k)]);
+            const uint32_t ln = at(k);
             const int tn = ln == old ? t_old : (ln == nw ? t_new : (int)a.cell_type[ln]);
             if (ln != old)
                 delta = __fsub_rn(delta, a.t.contact[t_old * a.n_types + tn]);
@@ -1218,7 +1247,7 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const PassVi
                 ++like_new;
         }
     }
-    if (old != 0 && like_old == 0 && !direct_keeps_other_colour<CG>(a, v.colour, old)) return;
+    if (old != 0 && like_old == 0 && !acc.keeps_other_colour(old)) return;
     const int ds_old = 2 * like_old - NOFF;
     const int ds_new = NOFF - 2 * like_new;
     int dv, ds;
@@ -1256,17 +1285,11 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const PassVi
             delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(d, __fadd_rn(__fmul_rn(2.0f, e), d))));
         }
     }
-    const float u = to_f32(draw(v.key_accept, target));
+    const float u = to_f32(draw(key_accept, target));
     if (!(delta <= 0.0f || u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
-    a.labels[target] = nw;
-    if (old != 0) {
-        atomicAdd(&v.vs_cur[old], pack_delta(-1, ds_old));
-        atomicSub(&a.vol_by_colour[(size_t)old * a.g.ncol + v.colour], 1);
-    }
-    if (nw != 0) {
-        atomicAdd(&v.vs_cur[nw], pack_delta(1, ds_new));
-        atomicAdd(&a.vol_by_colour[(size_t)nw * a.g.ncol + v.colour], 1);
-    }
+    acc.put(target, x, y, z, nw);
+    if (old != 0) acc.tally(old, -1, ds_old);
+    if (nw != 0) acc.tally(nw, 1, ds_new);
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
@@ -1277,7 +1300,9 @@ __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < targets) {
         const PassView v{a.colour, a.key_pick, a.key_accept, a.vs_base, a.vs_prev, a.vs_cur};
-        direct_target<DIM, NOFF, UNIFORM, false>(a, v, j);
+        int x, y, z;
+        direct_site<DIM>(a, a.colour, j, x, y, z);
+        direct_target<DIM, NOFF, UNIFORM>(a, GlobalPass<false>{a, v}, v.key_pick, v.key_accept, x, y, z);
     }
     rotate_tallies<DIM>(a);
 }
@@ -1336,7 +1361,11 @@ __global__ void __launch_bounds__(256) resident_sweep_kernel(const __grid_consta
             const long long p = r.pass0 + (long long)m * a.g.ncol + c;
             const PassView v{c, stream_key(r.seed, step, c, 0), stream_key(r.seed, step, c, 1), r.vs_base[p % 2],
                              r.vs_delta[(p + 2) % 3], reinterpret_cast<unsigned long long *>(r.vs_delta[p % 3])};
-            if (j < targets) direct_target<DIM, NOFF, UNIFORM, true>(a, v, j);
+            if (j < targets) {
+                int x, y, z;
+                direct_site<DIM>(a, c, j, x, y, z);
+                direct_target<DIM, NOFF, UNIFORM>(a, GlobalPass<true>{a, v}, v.key_pick, v.key_accept, x, y, z);
+            }
             // the rotation for the next pass, which no thread of this one reads
             int2 *next_base = r.vs_base[(p + 1) % 2];
             long long *clear = r.vs_delta[(p + 1) % 3];
@@ -1403,6 +1432,209 @@ cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream) 
         }
     return r.a.uniform_type >= 0 && r.a.uniform_contact_exact ? resident_any<true>(r, stream)
                                                               : resident_any<false>(r, stream);
+}
+
+// ---------------------------------------------------------------- the cluster sweep
+//
+// A small plane of a model the resident sweep takes runs every MCS of a call
+// in ONE thread-block cluster: the lattice split by rows over the cluster's
+// CTAs and held in their shared memory, the tallies dealt by label (label l
+// in CTA l mod C), every read or atomic on another CTA's part through
+// distributed shared memory, and the cluster's hardware barrier between
+// passes. The copies, draws and tally rotation are the resident sweep's;
+// the lattice and tallies go back to global memory at the end.
+
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterMax = 16;
+constexpr int kClusterSmem = 200 * 1024;
+
+// Shared-memory layout of one CTA of a C-CTA cluster sweep (bytes from the
+// start): delta[3][Lc] (i64), base[2][Lc] (int2), the pointer tables
+// (delta 3C, base 2C, volc C), rows[H], slab[R W] (u32), volc[Lc][4] (i32).
+struct ClusterLayout {
+    int C, R, Lc;
+    size_t delta, base, dptr, bptr, vptr, rows, slab, volc, bytes;
+    __host__ __device__ ClusterLayout(int w, int h, int n_labels, int c) : C(c) {
+        R = (h + c - 1) / c;
+        Lc = (n_labels + c - 1) / c;
+        delta = 0;
+        base = delta + 3 * (size_t)Lc * 8;
+        dptr = base + 2 * (size_t)Lc * 8;
+        bptr = dptr + 3 * (size_t)c * 8;
+        vptr = bptr + 2 * (size_t)c * 8;
+        rows = vptr + (size_t)c * 8;
+        slab = rows + (size_t)h * 8;
+        volc = slab + ((size_t)R * w * 4 + 15) / 16 * 16;
+        bytes = volc + (size_t)Lc * 16;
+    }
+};
+
+// Labels and tallies of a cluster pass: `rows[y]` is row y in whichever CTA
+// holds it; a label's tallies sit in CTA l & mask at index l >> shift.
+struct ClusterPass {
+    uint32_t *const *rows;
+    int2 *const *bptr;         // [slot * C + rank]
+    long long *const *dptr;    // [slot * C + rank]
+    int *const *vptr;          // [rank]
+    int C, shift, mask, colour, bslot, pslot, cslot;
+    __device__ __forceinline__ uint32_t label(int x, int y, int) const { return rows[y][x]; }
+    __device__ __forceinline__ int2 base(uint32_t l) const { return bptr[bslot * C + (l & mask)][l >> shift]; }
+    __device__ __forceinline__ long long prev(uint32_t l) const { return dptr[pslot * C + (l & mask)][l >> shift]; }
+    __device__ __forceinline__ bool keeps_other_colour(uint32_t old) const {
+        const int *v = vptr[old & mask] + (size_t)(old >> shift) * 4;
+        int other = 0;
+        for (int c = 0; c < 4; ++c)
+            if (c != colour) other += v[c];
+        return other != 0;
+    }
+    __device__ __forceinline__ void put(uint32_t, int x, int y, int, uint32_t nw) const { rows[y][x] = nw; }
+    __device__ __forceinline__ void tally(uint32_t l, int dv, int ds) const {
+        atomicAdd(reinterpret_cast<unsigned long long *>(&dptr[cslot * C + (l & mask)][l >> shift]),
+                  pack_delta(dv, ds));
+        atomicAdd(&vptr[l & mask][(size_t)(l >> shift) * 4 + colour], dv);
+    }
+};
+
+template <int NOFF, bool UNIFORM>
+__global__ void __launch_bounds__(kClusterThreads, 1) cluster_sweep_kernel(const __grid_constant__ ResidentLaunch r) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const SweepLaunch &a = r.a;
+    const int C = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
+    const int W = a.g.w, H = a.g.h, n_labels = a.n_labels;
+    const ClusterLayout L(W, H, n_labels, C);
+    const int tid = threadIdx.x, nth = blockDim.x;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    long long *delta = reinterpret_cast<long long *>(smem_raw + L.delta);
+    int2 *base = reinterpret_cast<int2 *>(smem_raw + L.base);
+    long long **dptr = reinterpret_cast<long long **>(smem_raw + L.dptr);
+    int2 **bptr = reinterpret_cast<int2 **>(smem_raw + L.bptr);
+    int **vptr = reinterpret_cast<int **>(smem_raw + L.vptr);
+    uint32_t **rows = reinterpret_cast<uint32_t **>(smem_raw + L.rows);
+    uint32_t *slab = reinterpret_cast<uint32_t *>(smem_raw + L.slab);
+    int *volc = reinterpret_cast<int *>(smem_raw + L.volc);
+    const int y0 = rank * L.R, y1 = min(H, y0 + L.R);
+
+    // this CTA's rows and labels, and where every CTA's parts lie
+    for (int i = tid; i < (y1 - y0) * W; i += nth) slab[i] = a.labels[(size_t)y0 * W + i];
+    for (int i = tid; i < L.Lc; i += nth) {
+        const int l = i * C + rank;
+        const bool in = l < n_labels;
+        for (int k = 0; k < 2; ++k) base[k * L.Lc + i] = in ? r.vs_base[k][l] : make_int2(0, 0);
+        for (int k = 0; k < 3; ++k) delta[k * L.Lc + i] = in ? r.vs_delta[k][l] : 0;
+        for (int c = 0; c < 4; ++c) volc[i * 4 + c] = in ? a.vol_by_colour[(size_t)l * 4 + c] : 0;
+    }
+    for (int y = tid; y < H; y += nth) {
+        const int o = y / L.R;
+        rows[y] = cluster.map_shared_rank(slab, o) + (size_t)(y - o * L.R) * W;
+    }
+    for (int i = tid; i < C; i += nth) {
+        for (int k = 0; k < 3; ++k) dptr[k * C + i] = cluster.map_shared_rank(delta + k * L.Lc, i);
+        for (int k = 0; k < 2; ++k) bptr[k * C + i] = cluster.map_shared_rank(base + k * L.Lc, i);
+        vptr[i] = cluster.map_shared_rank(volc, i);
+    }
+    cluster.sync();  // every CTA's part in place before any is read
+
+    const int hw = W / 2;
+    for (int m = 0; m < r.mcs; ++m) {
+        const int32_t step = (int32_t)((uint32_t)r.step0 + (uint32_t)m);
+        for (int c = 0; c < 4; ++c) {
+            const long long p = r.pass0 + (long long)m * 4 + c;
+            const ClusterPass acc{rows, bptr, dptr, vptr, C, __ffs(C) - 1, C - 1, c,
+                                  (int)(p % 2), (int)((p + 2) % 3), (int)(p % 3)};
+            const uint64_t key_pick = stream_key(r.seed, step, c, 0), key_accept = stream_key(r.seed, step, c, 1);
+            // this CTA's targets of colour c: rows of its slab of the colour's parity
+            const int yf = y0 + ((y0 & 1) != ((c >> 1) & 1));
+            const int count = yf < y1 ? (y1 - yf + 1) / 2 * hw : 0;
+            for (int t = tid; t < count; t += nth) {
+                const int y = yf + 2 * (t / hw), x = 2 * (t % hw) + (c & 1);
+                direct_target<2, NOFF, UNIFORM>(a, acc, key_pick, key_accept, x, y, 0);
+            }
+            // this CTA's labels' rotation for the next pass, which no thread of this one reads
+            int2 *next_base = base + ((p + 1) % 2) * L.Lc;
+            long long *clear = delta + ((p + 1) % 3) * L.Lc;
+            for (int i = tid; i < L.Lc; i += nth) {
+                int dv, ds;
+                unpack_delta(delta[acc.pslot * L.Lc + i], dv, ds);
+                const int2 b = base[acc.bslot * L.Lc + i];
+                next_base[i] = make_int2(b.x + dv, b.y + ds);
+                clear[i] = 0;
+            }
+            cluster.sync();
+        }
+    }
+
+    // back to global memory: this CTA's rows and labels
+    for (int i = tid; i < (y1 - y0) * W; i += nth) a.labels[(size_t)y0 * W + i] = slab[i];
+    for (int i = tid; i < L.Lc; i += nth) {
+        const int l = i * C + rank;
+        if (l >= n_labels) continue;
+        for (int k = 0; k < 2; ++k) r.vs_base[k][l] = base[k * L.Lc + i];
+        for (int k = 0; k < 3; ++k) r.vs_delta[k][l] = delta[k * L.Lc + i];
+        for (int c = 0; c < 4; ++c) a.vol_by_colour[(size_t)l * 4 + c] = volc[i * 4 + c];
+    }
+}
+
+// Run `mcs` MCS of a small 2D lean model in one cluster; cudaErrorNotSupported
+// (nothing launched) when the plane or its labels do not fit one.
+template <int NOFF, bool UNIFORM>
+static cudaError_t launch_cluster(const ResidentLaunch &r, cudaStream_t stream) {
+    const SweepLaunch &a = r.a;
+    const long long targets = (long long)a.g.w * a.g.h / 4;
+    int want = 1;
+    while (want < kClusterMax && (long long)want * kClusterThreads < targets) want *= 2;
+    // a thread's targets price one after another: past one each the
+    // cooperative grid's wider spread is faster
+    if ((long long)want * kClusterThreads < targets) return cudaErrorNotSupported;
+    auto kernel = cluster_sweep_kernel<NOFF, UNIFORM>;
+    static bool ready = false;
+    if (!ready) {
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmem) ||
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) {
+            cudaGetLastError();
+            return cudaErrorNotSupported;
+        }
+        ready = true;
+    }
+    // the widest cluster up to `want` CTAs that the device schedules and whose parts fit
+    for (int C = want; C >= 1; C /= 2) {
+        if (C > a.g.h) continue;
+        const ClusterLayout L(a.g.w, a.g.h, a.n_labels, C);
+        if (L.bytes > (size_t)kClusterSmem) break;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(C);
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.dynamicSmemBytes = L.bytes;
+        cfg.stream = stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = C;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) != cudaSuccess || clusters < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        return cudaLaunchKernelEx(&cfg, kernel, r);
+    }
+    return cudaErrorNotSupported;
+}
+
+cudaError_t launch_cluster_sweep(const ResidentLaunch &r, cudaStream_t stream) {
+    const SweepLaunch &a = r.a;
+    if (a.g.dim != 2 || a.g.ncol != 4) return cudaErrorNotSupported;
+    for (int k = 0; k < a.g.n_off; ++k)
+        for (int axis = 0; axis < 3; ++axis) {
+            const int want = a.g.n_off == 4 ? neighbour_offset<2, 4>(k, axis) : neighbour_offset<2, 8>(k, axis);
+            if (a.g.off[k][axis] != want) return cudaErrorInvalidValue;
+        }
+    const bool uniform = a.uniform_type >= 0 && a.uniform_contact_exact;
+    if (a.g.n_off == 4) return uniform ? launch_cluster<4, true>(r, stream) : launch_cluster<4, false>(r, stream);
+    if (a.g.n_off == 8) return uniform ? launch_cluster<8, true>(r, stream) : launch_cluster<8, false>(r, stream);
+    return cudaErrorNotSupported;
 }
 
 template <int DIM, int NOFF, bool UNIFORM>

@@ -136,6 +136,22 @@ def _population():
     return tiled(m, 6, 6, 6), 40
 
 
+def _two_types_plane():
+    # 128 x 128, two cell types in a checker of cells and a medium border:
+    # per-type contact, volume and surface tables; a small plane that a
+    # cluster of four CTAs holds, rows and labels spread over them
+    from glazier_b200.blueprint import CellType, Model
+
+    m = Model(width=128, height=128, contact=[0.0, 16.0, 16.0, 16.0, 8.0, 12.0, 16.0, 12.0, 10.0],
+              types=[CellType(), CellType(target_volume=64.0, lambda_volume=2.0),
+                     CellType(target_volume=48.0, lambda_volume=1.0, target_surface=30.0, lambda_surface=0.1)],
+              temperature=10.0, neighbour_order=2, seed=29)
+    start = tiled(m, 8, 14, 14)
+    cell_type = np.asarray(start.cell_type).copy()
+    cell_type[1:] = 1 + (np.arange(1, cell_type.size) % 2)
+    return Start(m, start.labels, cell_type.astype(np.uint8)), 20
+
+
 def _chemotaxis_ramp():
     m = with_species(sheet_model(seed=21), [("attractant", 0.0, 0.0, 0.0)], [[0.0], [0.0]], [[0.0], [0.0]],
                      [[0.0], [4.0]])
@@ -170,28 +186,31 @@ CASES = {
     "nematic": _nematic,
     "nematic-volume": _nematic_volume,
     "chemotaxis-ramp": _chemotaxis_ramp,
+    "two-types-plane": _two_types_plane,
 }
 
 
-@pytest.mark.parametrize("kernel", ["resident", "direct", "lean", "general"])
+@pytest.mark.parametrize("kernel", ["cluster", "resident", "direct", "lean", "general"])
 @pytest.mark.parametrize("ctas", ["0", "3"])
 @pytest.mark.parametrize("tma", ["1", "0"])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, kernel, monkeypatch):
     """`ctas` 3 caps the sweep's persistent grid at three CTAs, so every CTA
     walks several tiles and every window buffer takes tensor copies; `kernel`
-    forces the lean models onto the resident (every MCS of a call in one
+    forces the lean models onto the cluster (a plane held in one thread-block
+    cluster's shared memory), the resident (every MCS of a call in one
     launch, for models with nothing between passes), the direct, the lean or
     the general kernel (models with other terms always take the general one)."""
-    if kernel in ("resident", "direct") and (tma == "0" or ctas == "3"):
+    if kernel in ("cluster", "resident", "direct") and (tma == "0" or ctas == "3"):
         pytest.skip("the resident and direct kernels stage nothing and have no persistent grid")
     made, steps = CASES[name]()
     start, fields = made if isinstance(made, tuple) else (made, None)
     monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
     monkeypatch.setenv("GLAZIER_SWEEP_CTAS", ctas)
     monkeypatch.setenv("GLAZIER_SWEEP_LEAN", "0" if kernel == "general" else "1")
-    monkeypatch.setenv("GLAZIER_SWEEP_DIRECT", "1" if kernel in ("resident", "direct") else "0")
-    monkeypatch.setenv("GLAZIER_SWEEP_RESIDENT", "1" if kernel == "resident" else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_DIRECT", "1" if kernel in ("cluster", "resident", "direct") else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_RESIDENT", "1" if kernel in ("cluster", "resident") else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_CLUSTER", "1" if kernel == "cluster" else "0")
     gpu = device.GpuSimulation.from_start(start, fields)
     replay = ReplayOracle.from_start(start, fields)
     for chunk in (1, steps - 1):
