@@ -734,17 +734,26 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     const char *lean_env = std::getenv("GLAZIER_SWEEP_LEAN");
     h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !h->has_external && !h->has_motility && !has_conn &&
               !(lean_env && lean_env[0] == '0');
-    // A lean model of at most 512^2 sites takes the direct kernel, whose
-    // latency is lower when a pass is a few tiles (GLAZIER_SWEEP_DIRECT=0:
-    // never, =1: at any size).
+    // A lean plane of at most 1024^2 sites, or volume of at most 256^3, takes
+    // the direct kernel: one thread per target reading the lattice through
+    // the caches beats the lean kernel's window ring there (per MCS, L2
+    // flushed: 0.035 against 0.040 ms at 1024^2, 0.51 against 0.91 ms at
+    // 256^3; at 2048^2 the lean kernel leads). GLAZIER_SWEEP_DIRECT=0: never,
+    // =1: at any size.
     const char *direct_env = std::getenv("GLAZIER_SWEEP_DIRECT");
     const int direct_mode = direct_env ? (direct_env[0] == '0' ? 0 : 1) : -1;
-    h->direct = h->lean && (direct_mode == 1 || (direct_mode == -1 && sites <= 512LL * 512LL));
+    const long long direct_most = g.dim == 2 ? 1024LL * 1024LL : 256LL * 256LL * 256LL;
+    h->direct = h->lean && (direct_mode == 1 || (direct_mode == -1 && sites <= direct_most));
     // With no fields, division or death there is nothing between colour
-    // passes: a direct model runs every MCS of a call in one cooperative
-    // launch (GLAZIER_SWEEP_RESIDENT=0: a launch per pass).
+    // passes: a direct plane of at most 512^2 sites runs every MCS of a call
+    // in one cooperative launch, which saves more launch time than its grid
+    // barrier costs (in a volume the barrier and its L2 reads lose to a
+    // launch per pass). GLAZIER_SWEEP_RESIDENT=0: a launch per pass, =1: one
+    // launch at any size or dimension.
     const char *resident_env = std::getenv("GLAZIER_SWEEP_RESIDENT");
-    h->resident = h->direct && ns == 0 && !h->has_pop && !(resident_env && resident_env[0] == '0');
+    const int resident_mode = resident_env ? (resident_env[0] == '0' ? 0 : 1) : -1;
+    h->resident = h->direct && ns == 0 && !h->has_pop &&
+                  (resident_mode == 1 || (resident_mode == -1 && g.dim == 2 && sites <= 512LL * 512LL));
     // A resident plane runs in one thread-block cluster when it fits one
     // (GLAZIER_SWEEP_CLUSTER=0: the cooperative grid instead).
     const char *cluster_env = std::getenv("GLAZIER_SWEEP_CLUSTER");

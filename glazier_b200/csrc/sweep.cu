@@ -1143,38 +1143,25 @@ struct PassView {
     unsigned long long *vs_cur;
 };
 
-// A global load that (CG) bypasses the SM's L1, for data other blocks wrote
-// since this kernel began: L1 is not coherent across SMs within a launch.
-template <bool CG, typename V>
-__device__ __forceinline__ V load(const V *p) {
-    if constexpr (CG)
-        return __ldcg(p);
-    else
-        return *p;
-}
-
 // The per-colour guard of keeps_other_colour, for a direct pass.
-template <bool CG>
 __device__ __noinline__ bool direct_keeps_other_colour(const SweepLaunch &a, int colour, uint32_t old) {
     int other = 0;
     for (int c = 0; c < a.g.ncol; ++c)
-        if (c != colour) other += load<CG>(&a.vol_by_colour[(size_t)old * a.g.ncol + c]);
+        if (c != colour) other += a.vol_by_colour[(size_t)old * a.g.ncol + c];
     return other != 0;
 }
 
-// Where a direct pass finds and puts labels and tallies: global memory, read
-// through L2 when CG (the resident kernel reads what other blocks wrote).
-template <bool CG>
+// Where a direct pass finds and puts labels and tallies: global memory.
 struct GlobalPass {
     const SweepLaunch &a;
     const PassView &v;
     __device__ __forceinline__ uint32_t label(int x, int y, int z) const {
-        return load<CG>(&a.labels[(z * a.g.h + y) * a.g.w + x]);
+        return a.labels[(z * a.g.h + y) * a.g.w + x];
     }
-    __device__ __forceinline__ int2 base(uint32_t l) const { return load<CG>(&v.vs_base[l]); }
-    __device__ __forceinline__ long long prev(uint32_t l) const { return load<CG>(&v.vs_prev[l]); }
+    __device__ __forceinline__ int2 base(uint32_t l) const { return v.vs_base[l]; }
+    __device__ __forceinline__ long long prev(uint32_t l) const { return v.vs_prev[l]; }
     __device__ __forceinline__ bool keeps_other_colour(uint32_t old) const {
-        return direct_keeps_other_colour<CG>(a, v.colour, old);
+        return direct_keeps_other_colour(a, v.colour, old);
     }
     __device__ __forceinline__ void put(uint32_t target, int, int, int, uint32_t nw) const { a.labels[target] = nw; }
     __device__ __forceinline__ void tally(uint32_t l, int dv, int ds) const {
@@ -1302,7 +1289,7 @@ __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant
         const PassView v{a.colour, a.key_pick, a.key_accept, a.vs_base, a.vs_prev, a.vs_cur};
         int x, y, z;
         direct_site<DIM>(a, a.colour, j, x, y, z);
-        direct_target<DIM, NOFF, UNIFORM>(a, GlobalPass<false>{a, v}, v.key_pick, v.key_accept, x, y, z);
+        direct_target<DIM, NOFF, UNIFORM>(a, GlobalPass{a, v}, v.key_pick, v.key_accept, x, y, z);
     }
     rotate_tallies<DIM>(a);
 }
@@ -1314,7 +1301,10 @@ __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant
 // cooperative launch: the direct pass's work per target, the tally rotation,
 // then a grid barrier, pass after pass. Each pass's draws and tally slots
 // follow from its number as the host would set them. Reads of what other
-// blocks wrote in earlier passes go to L2. The barrier's wait is bounded: a
+// blocks wrote in earlier passes are plain loads: the barrier's gpu-scope
+// release (each block's fence and arrival) and acquire (the waiting thread's
+// acquire load and fence, then the block barrier) order them after those
+// writes, whatever an SM's L1 held before. The barrier's wait is bounded: a
 // block that gives up sets error flag 4 and returns, and the others then
 // give up at their next barrier.
 
@@ -1364,15 +1354,15 @@ __global__ void __launch_bounds__(256) resident_sweep_kernel(const __grid_consta
             if (j < targets) {
                 int x, y, z;
                 direct_site<DIM>(a, c, j, x, y, z);
-                direct_target<DIM, NOFF, UNIFORM>(a, GlobalPass<true>{a, v}, v.key_pick, v.key_accept, x, y, z);
+                direct_target<DIM, NOFF, UNIFORM>(a, GlobalPass{a, v}, v.key_pick, v.key_accept, x, y, z);
             }
             // the rotation for the next pass, which no thread of this one reads
             int2 *next_base = r.vs_base[(p + 1) % 2];
             long long *clear = r.vs_delta[(p + 1) % 3];
             for (size_t l = j; l < (size_t)a.n_labels; l += stride) {
                 int dv, ds;
-                unpack_delta(__ldcg(&v.vs_prev[l]), dv, ds);
-                const int2 b = __ldcg(&v.vs_base[l]);
+                unpack_delta(v.vs_prev[l], dv, ds);
+                const int2 b = v.vs_base[l];
                 next_base[l] = make_int2(b.x + dv, b.y + ds);
                 clear[l] = 0;
             }
