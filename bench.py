@@ -477,35 +477,69 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+class Ranks:
+    """One process per GPU as torchrun starts them (RANK, WORLD_SIZE,
+    LOCAL_RANK, MASTER_* from the environment): a barrier and the max over
+    ranks, the only collectives the bench takes, since its replicas exchange
+    nothing. NCCL on the GPUs; gloo with CPU tensors for tests of the host
+    side. A short process-group timeout ends a wait on a rank that is gone."""
+
+    def __init__(self, backend: str = "nccl", timeout_s: float = 120.0):
+        import torch
+
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.cuda = backend == "nccl"
+        self.dist = None
+        if self.cuda:
+            torch.cuda.set_device(self.local if self.world > 1 else 0)
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+        self.device = torch.device("cuda", torch.cuda.current_device()) if self.cuda else torch.device("cpu")
+
+    def barrier(self) -> None:
+        import torch
+
+        if self.dist is not None:
+            self.dist.barrier()
+        if self.cuda:
+            torch.cuda.synchronize()
+
+    def max_over_ranks(self, x: float) -> float:
+        import torch
+
+        if self.dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_rate(units_per_rank: float, slowest_s: float, world: int) -> float:
+    """Units all ranks processed over the slowest rank's time: the
+    whole-job figure of a weakly scaled run."""
+    return units_per_rank * world / slowest_s
+
+
 def run_ours(args) -> None:
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(0)
-    dev = torch.device("cuda", torch.cuda.current_device())
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl")
+    world, rank, local = ranks.world, ranks.rank, ranks.local
+    dev = ranks.device
+    barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
     from glazier_b200.engine import GpuSimulation
 
@@ -530,7 +564,7 @@ def run_ours(args) -> None:
         barrier()
     total_ms = sweep_ms + field_ms + pop_ms
     slowest = max_over_ranks(total_ms)
-    value = sites * args.steps * world / (slowest / 1e3)
+    value = whole_job_rate(sites * args.steps, slowest / 1e3, world)
     launches_per_step = 4  # four colour passes; the workload has no fields and no population
 
     # end to end through the public API, host buffers pinned
@@ -547,7 +581,7 @@ def run_ours(args) -> None:
         sim.labels_to(pinned_out.data_ptr(), sites)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = sites * job_mcs * jobs * world / e2e_s
+    e2e_value = whole_job_rate(sites * job_mcs * jobs, e2e_s, world)
     assert int(pinned_out.max()) <= (args.size // 8) ** 2
 
     peak, peak_kind = measured_peak()
@@ -560,9 +594,7 @@ def run_ours(args) -> None:
                 "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3}
 
     sim.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank != 0:
         return
     line = {
