@@ -186,6 +186,51 @@ def ensemble_compare(mcs: int, device: int) -> dict:
             "lattices_identical": bool(same)}
 
 
+def mixed_ensemble_compare(mcs: int, device: int) -> dict:
+    """The configuration's full mix: 64 replicas alternating the plain
+    monolayer and the two-field infection model (sides log-uniform 128..1024,
+    own T, J and lambda_V; `mixed_ensemble_starts`). The monolayers run as
+    one batch, each infection model as its own engine beside it; against
+    looping the plain engine over the same replicas. Wall clock to every
+    replica's result, both ways; a batched and an infection replica compared
+    for identity."""
+    import torch
+
+    from glazier_b200.engine import GpuSimulation
+    from glazier_b200.ensemble import Ensemble
+    from glazier_b200.workloads import INFECTION_RULE, mixed_ensemble_starts
+
+    starts, infected = mixed_ensemble_starts(64)
+    sites = sum(st.model.sites for st in starts)
+    ens = Ensemble(starts, device=device)
+    for i in infected:
+        ens.set_infection(i, *INFECTION_RULE)
+    ens.autotune(3)
+    ens.step(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ens.step(mcs)
+    mixed_s = time.perf_counter() - t0
+    sims = [GpuSimulation.from_start(st, device=device) for st in starts]
+    for i in infected:
+        sims[i].set_infection(*INFECTION_RULE)
+    for sim in sims:
+        sim.step(3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sim in sims:
+        sim.step(mcs)
+    looped_s = time.perf_counter() - t0
+    same = all(np.array_equal(ens.labels(i), sims[i].labels()) for i in (0, infected[0], infected[-1]))
+    for sim in sims:
+        sim.close()
+    ens.close()
+    return {"replicas": 64, "infection_replicas": len(infected), "sites": sites, "mcs": mcs, "mixed_s": mixed_s,
+            "looped_plain_s": looped_s, "speedup": looped_s / mixed_s, "lattices_identical": bool(same),
+            "note": "monolayers batched in one persistent launch per colour; infection models as engines on their "
+                    "own streams beside it"}
+
+
 def adjoint_compare(steps: int, every: int, repeats: int, device: int) -> dict:
     """The field adjoint at 512^2 (4096 cells, two fields, four types): record
     `steps` MCS of owners from the engine, then time the adjoint's forward and
@@ -611,6 +656,7 @@ def run_ours(args) -> None:
     }
     if world == 1 and not args.no_ensemble:
         line["ensemble"] = ensemble_compare(100, torch.cuda.current_device())
+        line["mixed_ensemble"] = mixed_ensemble_compare(100, torch.cuda.current_device())
     if world == 1 and not args.no_published:
         line["volume"] = volume_leg(20, torch.cuda.current_device(), peak)
         line["published_rows"] = published_rows(torch.cuda.current_device())

@@ -157,6 +157,10 @@ def _declare_extras(L) -> None:
     L.glz_ens_create.restype = C.c_int
     L.glz_ens_create.argtypes = [C.c_int, C.POINTER(GlzModel), C.POINTER(_P), C.POINTER(_P), C.POINTER(C.c_size_t),
                                  C.POINTER(_P)]
+    L.glz_ens_n_labels.restype = C.c_size_t
+    L.glz_ens_n_labels.argtypes = [_P, C.c_int]
+    L.glz_ens_set_infection.restype = C.c_int
+    L.glz_ens_set_infection.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
     L.glz_ens_step.restype = C.c_int
     L.glz_ens_step.argtypes = [_P, C.c_uint64]
     L.glz_ens_step_timed.restype = C.c_int

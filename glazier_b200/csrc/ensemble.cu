@@ -17,11 +17,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/glazier_gpu.h"
@@ -134,6 +136,13 @@ struct glz_ens {
     int schedule = 0;  // 0: replicas in their own order; 1: largest first
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // Replicas as the caller numbered them: slot[i] >= 0 is replica i's index
+    // in the batch above (n of them), slot[i] < 0 engine -slot[i] - 1, a
+    // replica whose model states more than contact, volume and surface,
+    // stepped as its own engine beside the batch.
+    int all = 0, device = 0;
+    std::vector<int> slot;
+    std::vector<glz_gpu *> engines;
 };
 
 namespace {
@@ -249,8 +258,9 @@ int settle_all(glz_ens *h) {
 
 extern "C" {
 
-int glz_ens_create(int n, const glz_model *models, const uint32_t *const *labels, const uint8_t *const *cell_types,
-                   const size_t *n_labels, glz_ens **out) {
+// The batch: replicas whose models price contact, volume and surface only.
+static int create_batched(int n, const glz_model *models, const uint32_t *const *labels,
+                          const uint8_t *const *cell_types, const size_t *n_labels, glz_ens **out) {
     if (!out) return fail(GLZ_INVALID, "null output handle");
     *out = nullptr;
     if (n < 1 || !models || !labels || !cell_types || !n_labels) return fail(GLZ_INVALID, "no replicas or a null array");
@@ -463,18 +473,140 @@ int glz_ens_create(int n, const glz_model *models, const uint32_t *const *labels
     return GLZ_OK;
 }
 
+// Whether a model states a term the batch does not price: fields, length,
+// connectivity, division, death, motility, drift or nematic.
+static bool needs_engine(const glz_model &m) {
+    bool extra = m.n_species > 0;
+    for (int k = 0; k < m.n_types; ++k) {
+        extra |= at(m.lambda_length, k) != 0.0 || at(m.division_volume, k) > 0.0 || at(m.death_rate, k) > 0.0;
+        extra |= m.connected && m.connected[k];
+        extra |= at(m.lambda_activity, k) != 0.0 || (m.nematic && at(m.lambda_nematic, k) != 0.0);
+        for (int a = 0; a < 3; ++a) extra |= at(m.external, 3 * (size_t)k + a) != 0.0;
+    }
+    return extra;
+}
+
+int glz_ens_create(int n, const glz_model *models, const uint32_t *const *labels, const uint8_t *const *cell_types,
+                   const size_t *n_labels, glz_ens **out) {
+    if (!out) return fail(GLZ_INVALID, "null output handle");
+    *out = nullptr;
+    if (n < 1 || !models || !labels || !cell_types || !n_labels) return fail(GLZ_INVALID, "no replicas or a null array");
+    std::vector<int> batch, alone;
+    for (int r = 0; r < n; ++r) (needs_engine(models[r]) ? alone : batch).push_back(r);
+    glz_ens *h = nullptr;
+    if (!batch.empty()) {
+        std::vector<glz_model> bm;
+        std::vector<const uint32_t *> bl;
+        std::vector<const uint8_t *> bt;
+        std::vector<size_t> bn;
+        for (int r : batch) {
+            bm.push_back(models[r]);
+            bl.push_back(labels[r]);
+            bt.push_back(cell_types[r]);
+            bn.push_back(n_labels[r]);
+        }
+        if (int rc = create_batched((int)batch.size(), bm.data(), bl.data(), bt.data(), bn.data(), &h)) return rc;
+    } else {
+        h = new glz_ens();
+        h->n = 0;
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            glz_ens_destroy(h);
+            return fail(GLZ_DRIVER, "cannot create a stream");
+        }
+    }
+    h->all = n;
+    h->slot.assign(n, 0);
+    cudaGetDevice(&h->device);
+    for (size_t b = 0; b < batch.size(); ++b) h->slot[batch[b]] = (int)b;
+    for (int r : alone) {
+        glz_gpu *g = nullptr;
+        if (int rc = glz_gpu_create(&models[r], labels[r], cell_types[r], n_labels[r], nullptr, nullptr, &g)) {
+            const std::string why = glz_last_error();
+            glz_ens_destroy(h);
+            return fail(rc, "replica " + std::to_string(r) + ": " + why);
+        }
+        h->engines.push_back(g);
+        h->slot[r] = -(int)h->engines.size();
+    }
+    *out = h;
+    return GLZ_OK;
+}
+
+// Replica i: its batch index (>= 0) or its engine, GLZ_INVALID when there is none.
+static int which(glz_ens *h, int replica, int *batched, glz_gpu **engine) {
+    if (replica < 0 || replica >= h->all) return fail(GLZ_INVALID, "no such replica");
+    const int s = h->slot[replica];
+    *batched = s >= 0 ? s : -1;
+    *engine = s < 0 ? h->engines[-s - 1] : nullptr;
+    return GLZ_OK;
+}
+
+// `steps` MCS of every replica: the batch on the ensemble's stream, each
+// engine on its own stream from a host thread of its own, all at once.
+static int step_all(glz_ens *h, uint64_t steps, double *ms) {
+    if (h->engines.empty()) return run(h, steps, true, ms);
+    const auto t0 = std::chrono::steady_clock::now();
+    const size_t e = h->engines.size();
+    std::vector<int> rcs(e, GLZ_OK);
+    std::vector<std::string> why(e);
+    std::vector<std::thread> threads;
+    threads.reserve(e);
+    for (size_t k = 0; k < e; ++k)
+        threads.emplace_back([h, k, steps, &rcs, &why] {
+            if (cudaSetDevice(h->device) != cudaSuccess) {
+                rcs[k] = GLZ_DRIVER;
+                why[k] = "cannot select the ensemble's device";
+                return;
+            }
+            rcs[k] = glz_gpu_step(h->engines[k], steps);
+            if (rcs[k]) why[k] = glz_last_error();
+        });
+    int rc = GLZ_OK;
+    if (h->n > 0)
+        rc = run(h, steps, true, nullptr);
+    else
+        h->step += (long long)steps;
+    for (auto &t : threads) t.join();
+    if (ms) *ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (rc) return rc;
+    for (int r = 0; r < h->all; ++r)
+        if (h->slot[r] < 0 && rcs[-h->slot[r] - 1])
+            return fail(rcs[-h->slot[r] - 1], "replica " + std::to_string(r) + ": " + why[-h->slot[r] - 1]);
+    return GLZ_OK;
+}
+
 int glz_ens_step(glz_ens *h, uint64_t steps) {
     if (!h) return fail(GLZ_INVALID, "null handle");
-    return run(h, steps, true, nullptr);
+    return step_all(h, steps, nullptr);
 }
 
 int glz_ens_step_timed(glz_ens *h, uint64_t steps, double *ms) {
     if (!h || !ms) return fail(GLZ_INVALID, "null handle or output");
-    return run(h, steps, true, ms);
+    return step_all(h, steps, ms);
+}
+
+size_t glz_ens_n_labels(glz_ens *h, int replica) {
+    int b = -1;
+    glz_gpu *g = nullptr;
+    if (!h || which(h, replica, &b, &g)) return 0;
+    return g ? glz_gpu_n_labels(g) : h->reps[b].n_labels;
+}
+
+int glz_ens_set_infection(glz_ens *h, int replica, int species, int from_type, int to_type, double threshold) {
+    if (!h) return fail(GLZ_INVALID, "null handle");
+    int b = -1;
+    glz_gpu *g = nullptr;
+    if (int rc = which(h, replica, &b, &g)) return rc;
+    if (!g) return fail(GLZ_UNSUPPORTED, "replica " + std::to_string(replica) + " is batched and has no fields");
+    return glz_gpu_set_infection(g, species, from_type, to_type, threshold);
 }
 
 int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice) {
     if (!h) return fail(GLZ_INVALID, "null handle");
+    if (h->n == 0) {  // nothing batched: no schedule to choose
+        if (choice) *choice = 0;
+        return GLZ_OK;
+    }
     if (trial_steps < 1) trial_steps = 1;
     // Snapshot the state, time each candidate on it, put the state back: the
     // candidates give identical results, so only the time decides.
@@ -532,12 +664,14 @@ int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice) {
 int glz_ens_set_schedule(glz_ens *h, int schedule, int max_ctas) {
     if (!h) return fail(GLZ_INVALID, "null handle");
     if (schedule < 0 || schedule > 1 || max_ctas < 0) return fail(GLZ_INVALID, "no such schedule");
-    return set_schedule(h, schedule, max_ctas);
+    return h->n > 0 ? set_schedule(h, schedule, max_ctas) : GLZ_OK;
 }
 
 int glz_ens_labels(glz_ens *h, int replica, uint32_t *out, size_t sites) {
     if (!h || !out) return fail(GLZ_INVALID, "null handle or buffer");
-    if (replica < 0 || replica >= h->n) return fail(GLZ_INVALID, "no such replica");
+    glz_gpu *g = nullptr;
+    if (int rc = which(h, replica, &replica, &g)) return rc;
+    if (g) return glz_gpu_labels(g, out, sites);
     const Replica &rep = h->reps[replica];
     if (sites != (size_t)rep.g.sites) return fail(GLZ_INVALID, "the buffer is not one label per site");
     CU(cudaMemcpyAsync(out, h->labels + rep.label_off, sites * 4, cudaMemcpyDeviceToHost, h->stream));
@@ -560,7 +694,9 @@ static int ens_tallies(glz_ens *h, int replica, std::vector<int2> &vs, unsigned 
 
 int glz_ens_volumes(glz_ens *h, int replica, uint32_t *out, size_t *count) {
     if (!h || !count) return fail(GLZ_INVALID, "null handle or count");
-    if (replica < 0 || replica >= h->n) return fail(GLZ_INVALID, "no such replica");
+    glz_gpu *g = nullptr;
+    if (int rc = which(h, replica, &replica, &g)) return rc;
+    if (g) return glz_gpu_volumes(g, out, count);
     const size_t n = h->reps[replica].n_labels;
     if (!out || *count < n) {
         *count = n;
@@ -577,7 +713,9 @@ int glz_ens_volumes(glz_ens *h, int replica, uint32_t *out, size_t *count) {
 
 int glz_ens_surfaces(glz_ens *h, int replica, int64_t *out, size_t *count) {
     if (!h || !count) return fail(GLZ_INVALID, "null handle or count");
-    if (replica < 0 || replica >= h->n) return fail(GLZ_INVALID, "no such replica");
+    glz_gpu *g = nullptr;
+    if (int rc = which(h, replica, &replica, &g)) return rc;
+    if (g) return glz_gpu_surfaces(g, out, count);
     const size_t n = h->reps[replica].n_labels;
     if (!out || *count < n) {
         *count = n;
@@ -598,6 +736,7 @@ void *glz_ens_stream(glz_ens *h) { return h ? (void *)h->stream : nullptr; }
 
 void glz_ens_destroy(glz_ens *h) {
     if (!h) return;
+    for (glz_gpu *g : h->engines) glz_gpu_destroy(g);
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graph(h);
     cudaFree(h->labels); cudaFree(h->cell_type);

@@ -1,8 +1,10 @@
 """A batch of independent Cellular Potts replicas run as one on the B200.
 
-The Python face of the ``glz_ens_*`` entry points: every replica's tiles go
-through one persistent launch per colour, and one Monte Carlo step is
-replayed from a CUDA graph. Each replica's results are bit-identical to a
+The Python face of the ``glz_ens_*`` entry points: every replica whose model
+prices contact, volume and surface only goes through one persistent launch
+per colour, one Monte Carlo step replayed from a CUDA graph; a replica with
+fields, division, death or the other terms runs as its own engine beside the
+batch, at the same time. Each replica's results are bit-identical to a
 ``GpuSimulation`` run of the same start, so the schedule the autotuner picks
 changes only the time.
 """
@@ -19,7 +21,8 @@ from .engine import check
 
 class Ensemble:
     """Replicas given as ``glazier_b200.blueprint.Start`` objects (their
-    models may differ in size and parameters but share a neighbourhood)."""
+    models may differ in size, parameters and terms; the batched ones share a
+    neighbourhood)."""
 
     def __init__(self, starts, device: int | None = None):
         L = _lib.lib()
@@ -44,7 +47,6 @@ class Ensemble:
         self._h = h
         self.n = n
         self.sites = [st.model.sites for st in starts]
-        self.n_labels = [st.cell_type.size for st in starts]
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
@@ -62,6 +64,15 @@ class Ensemble:
 
     def __exit__(self, *exc):
         self.close()
+
+    def n_labels(self, i: int) -> int:
+        """Labels replica ``i`` has issued, the medium included."""
+        return int(_lib.lib().glz_ens_n_labels(self._h, int(i)))
+
+    def set_infection(self, i: int, species: int, from_type: int, to_type: int, threshold: float) -> None:
+        """The infection rule for replica ``i`` (``GpuSimulation.set_infection``)."""
+        check(_lib.lib().glz_ens_set_infection(self._h, int(i), int(species), int(from_type), int(to_type),
+                                               float(threshold)))
 
     def step(self, steps: int = 1) -> None:
         check(_lib.lib().glz_ens_step(self._h, int(steps)))
@@ -90,13 +101,13 @@ class Ensemble:
         return out
 
     def volumes(self, i: int) -> np.ndarray:
-        n = C.c_size_t(self.n_labels[i])
+        n = C.c_size_t(self.n_labels(i))
         out = np.empty(n.value, dtype=np.uint32)
         check(_lib.lib().glz_ens_volumes(self._h, int(i), _lib.ptr(out), C.byref(n)))
         return out
 
     def surfaces(self, i: int) -> np.ndarray:
-        n = C.c_size_t(self.n_labels[i])
+        n = C.c_size_t(self.n_labels(i))
         out = np.empty(n.value, dtype=np.int64)
         check(_lib.lib().glz_ens_surfaces(self._h, int(i), _lib.ptr(out), C.byref(n)))
         return out

@@ -92,6 +92,36 @@ def ensemble_starts(count: int = 64, seed: int = 1, side: int = 8, low: int = 12
     return starts
 
 
+def mixed_ensemble_starts(count: int = 64, seed: int = 1, side: int = 8, low: int = 128, high: int = 1024) -> list:
+    """`count` replicas alternating the plain monolayer (even places, as
+    `ensemble_starts` draws them) and the two-field infection model (odd
+    places: `infection_start` on a lattice of the drawn side, a centred block
+    of cells covering half of it, 32 immune cells, with the drawn temperature,
+    cell-cell contact energy and epithelial volume constraint). The infection
+    replicas take INFECTION_RULE. Returns (starts, indices of the infection
+    replicas)."""
+    plain = ensemble_starts(count, seed, side, low, high)
+    starts, infected = [], []
+    for i, st in enumerate(plain):
+        if i % 2 == 0:
+            starts.append(st)
+            continue
+        size = st.model.width
+        inf = infection_start(seed=(seed * 1_000_003 + i) & _M64, size=size, side=side, grid=size // (2 * side))
+        m = inf.model
+        u = [uniform01(seed, i, k) for k in range(4)]
+        m.temperature = 5.0 + 15.0 * u[1]
+        j = 6.0 + round(10.0 * u[2] * 64) / 64
+        n = m.n_types
+        m.contact = [j if (a != 0 and b != 0) else m.contact[a * n + b] for a in range(n) for b in range(n)]
+        for t in (1, 2):
+            m.types[t].lambda_volume = 0.5 + 1.5 * u[3]
+        m.validate()
+        starts.append(inf)
+        infected.append(i)
+    return starts, infected
+
+
 def adjoint_start(seed: int = 1, size: int = 512, side: int = 8) -> Start:
     """The field-adjoint workload: a periodic `size` lattice tiled by cells of
     `side` (512^2: 4096 cells), types medium, healthy, infected and immune,

@@ -179,14 +179,16 @@ void glz_gpu_destroy(glz_gpu *h);
 
 /* ---------------------------------------------------------------- ensemble
  *
- * A batch of independent replicas run as one: every replica's tiles in one
- * persistent launch per colour, one Monte Carlo step replayed from a CUDA
- * graph. No reference counterpart (glazier runs one lattice per
- * GpuSimulation); each replica's results are bit-identical to a glz_gpu_*
- * run of the same start. Replicas may differ in size, parameters and seed but
- * share one neighbourhood; the ensemble runs the contact, volume and surface
- * terms and refuses models with fields, length, connectivity, population,
- * motility, drift or nematic terms (GLZ_UNSUPPORTED).
+ * A batch of independent replicas run as one: every replica whose model
+ * prices contact, volume and surface only has its tiles in one persistent
+ * launch per colour, one Monte Carlo step replayed from a CUDA graph; a
+ * replica whose model states more (fields, length, connectivity, division,
+ * death, motility, drift, nematic) runs as its own engine beside the batch,
+ * on its own stream from a host thread of its own, over the same steps. No
+ * reference counterpart (glazier runs one lattice per GpuSimulation); each
+ * replica's results are bit-identical to a glz_gpu_* run of the same start.
+ * Replicas may differ in size, parameters and seed; the batched ones share
+ * one neighbourhood.
  */
 typedef struct glz_ens glz_ens;
 
@@ -196,8 +198,15 @@ int glz_ens_create(int n, const glz_model *models, const uint32_t *const *labels
                    const size_t *n_labels, glz_ens **out);
 /* Run `steps` Monte Carlo steps of every replica and wait. */
 int glz_ens_step(glz_ens *h, uint64_t steps);
-/* The same, reporting the device milliseconds the steps took. */
+/* The same, reporting the milliseconds the steps took: the batch's device
+ * time, or the call's elapsed time when engine replicas run beside it. */
 int glz_ens_step_timed(glz_ens *h, uint64_t steps, double *ms);
+/* Labels replica `replica` has issued so far, the medium included (an engine
+ * replica's count grows with its divisions); 0 for no such replica. */
+size_t glz_ens_n_labels(glz_ens *h, int replica);
+/* glz_gpu_set_infection for an engine replica; a batched replica has no
+ * fields (GLZ_UNSUPPORTED). */
+int glz_ens_set_infection(glz_ens *h, int replica, int species, int from_type, int to_type, double threshold);
 /* Time each schedule (replica order x persistent grid) on a snapshot of the
  * state for `trial_steps` steps, restore the state, keep the fastest. */
 int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice);

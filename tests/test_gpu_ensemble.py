@@ -11,6 +11,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+from conftest import sheet_model, tiled
 from glazier_b200.blueprint import Start
 from glazier_b200.workloads import ensemble_starts, monolayer
 from oracle.replay import ReplayOracle
@@ -96,14 +97,73 @@ def test_autotuning_leaves_the_run_where_it_was(device):
         assert np.array_equal(ens.volumes(i), ref.volumes(i)), f"replica {i}"
 
 
+def _plain_with_rule(device, start, steps, rule):
+    sim = device.GpuSimulation.from_start(start)
+    if rule is not None:
+        sim.set_infection(*rule)
+    sim.step(steps)
+    out = sim.labels(), sim.volumes(), sim.surfaces(), sim.n_labels
+    sim.close()
+    return out
+
+
+def test_replicas_with_more_terms_run_beside_the_batch_and_match_their_plain_runs(device):
+    # three batched monolayers, an infection model (fields, division, death,
+    # length, chemotaxis, connectivity) and a dividing sheet that run as their
+    # own engines at the same time
+    from glazier_b200.ensemble import Ensemble
+    from glazier_b200.workloads import INFECTION_RULE, infection_start
+
+    # 36-site cells with room around them, growing toward 100 sites and
+    # dividing at 48 (the parity suite's population sheet)
+    dividing = tiled(sheet_model(seed=77, division_volume=48.0, death_rate=0.01, target_volume=100.0), 6, 6, 6)
+    starts = _starts()[:3] + [infection_start(seed=5, size=128, grid=6, immune=4), dividing]
+    rules = [None, None, None, INFECTION_RULE, None]
+    ens = Ensemble(starts)
+    ens.set_infection(3, *INFECTION_RULE)
+    ens.autotune(2)
+    ens.step(4)
+    ens.step(26)
+    assert ens.mcs == 30
+    for i, (st, rule) in enumerate(zip(starts, rules)):
+        labels, volumes, surfaces, n_labels = _plain_with_rule(device, st, 30, rule)
+        assert ens.n_labels(i) == n_labels, f"replica {i}"
+        assert np.array_equal(ens.labels(i), labels), f"replica {i}"
+        assert np.array_equal(ens.volumes(i), volumes), f"replica {i}"
+        assert np.array_equal(ens.surfaces(i), surfaces), f"replica {i}"
+    assert ens.n_labels(4) > starts[4].cell_type.size  # the sheet divided
+    ens.close()
+
+
+def test_an_ensemble_of_engine_replicas_alone_runs(device):
+    from glazier_b200.ensemble import Ensemble
+    from glazier_b200.workloads import INFECTION_RULE, infection_start
+
+    starts = [infection_start(seed=s, size=96, grid=4, immune=3) for s in (1, 2)]
+    ens = Ensemble(starts)
+    for i in range(2):
+        ens.set_infection(i, *INFECTION_RULE)
+    assert ens.autotune(2) == 0
+    ens.step(10)
+    assert ens.mcs == 10
+    for i, st in enumerate(starts):
+        labels, volumes, _, _ = _plain_with_rule(device, st, 10, INFECTION_RULE)
+        assert np.array_equal(ens.labels(i), labels)
+        assert np.array_equal(ens.volumes(i), volumes)
+    ens.close()
+
+
 def test_the_ensemble_refuses_what_it_does_not_run(device):
     from glazier_b200.engine import GpuError
     from glazier_b200.ensemble import Ensemble
+    from glazier_b200.workloads import INFECTION_RULE
 
-    starts = _starts()[:2]
-    starts[1].model.types[1].division_volume = 100.0
-    with pytest.raises(GpuError, match="contact, volume and surface"):
-        Ensemble(starts)
+    ens = Ensemble(_starts()[:2])
+    with pytest.raises(GpuError, match="batched and has no fields"):
+        ens.set_infection(0, *INFECTION_RULE)
+    with pytest.raises(GpuError, match="no such replica"):
+        ens.labels(2)
+    ens.close()
     odd = monolayer(64)
     odd.model.width = 66
     odd = Start.tiled(odd.model, 8)
