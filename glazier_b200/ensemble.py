@@ -16,7 +16,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .engine import check
+from .engine import GpuError, check
 
 
 class Ensemble:
@@ -95,7 +95,13 @@ class Ensemble:
     def mcs(self) -> int:
         return int(_lib.lib().glz_ens_mcs(self._h))
 
+    def _replica(self, i: int) -> int:
+        if not 0 <= int(i) < self.n:
+            raise GpuError(_lib.GLZ_INVALID, f"no such replica: {i} of {self.n}")
+        return int(i)
+
     def labels(self, i: int) -> np.ndarray:
+        i = self._replica(i)
         out = np.empty(self.sites[i], dtype=np.uint32)
         check(_lib.lib().glz_ens_labels(self._h, int(i), _lib.ptr(out), out.size))
         return out
