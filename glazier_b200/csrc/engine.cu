@@ -136,6 +136,7 @@ struct glz_gpu {
     bool use_tma = false;
     bool lean = false;    // the sweep prices contact, volume and surface only
     bool direct = false;  // ... on a lattice small enough for the direct kernel
+    bool compact = false; // ... queueing a warp's unlike copies (large passes)
     bool resident = false;  // ... with nothing between passes: every MCS in one launch
     bool cluster = false;   // ... a plane, in one thread-block cluster's shared memory
     unsigned *barrier = nullptr;  // the resident sweep's grid barrier
@@ -387,6 +388,7 @@ glz::SweepLaunch pass_launch(glz_gpu *h, int colour) {
     a.use_tma = h->use_tma;
     a.lean = h->lean;
     a.direct = h->direct;
+    a.compact = h->compact;
     a.max_ctas = h->max_ctas;
     a.tensor_map = h->use_tma ? &h->tmap : nullptr;
     a.error_flag = h->error_flag;
@@ -744,6 +746,12 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     const int direct_mode = direct_env ? (direct_env[0] == '0' ? 0 : 1) : -1;
     const long long direct_most = g.dim == 2 ? 1024LL * 1024LL : 256LL * 256LL * 256LL;
     h->direct = h->lean && (direct_mode == 1 || (direct_mode == -1 && sites <= direct_most));
+    // From a million targets a pass the direct kernel queues each warp's
+    // unlike copies and prices them in full rounds (GLAZIER_SWEEP_COMPACT=1:
+    // at any size, =0: never).
+    const char *compact_env = std::getenv("GLAZIER_SWEEP_COMPACT");
+    const int compact_mode = compact_env ? (compact_env[0] == '0' ? 0 : 1) : -1;
+    h->compact = compact_mode == 1 || (compact_mode == -1 && sites / g.ncol >= glz::kDirectCompactFrom);
     // With no fields, division or death there is nothing between colour
     // passes: a direct plane of at most 512^2 sites runs every MCS of a call
     // in one cooperative launch, which saves more launch time than its grid

@@ -95,6 +95,7 @@ struct SweepLaunch {
     int use_tma;
     int lean;                // take the lean kernel: no length, chemotaxis, connectivity or moment tracking
     int direct;              // a lean model small enough for the direct kernel (one thread per target)
+    int compact;             // the direct kernel queues a warp's unlike copies before pricing them
     int max_ctas;            // > 0 caps the persistent grid (each CTA then walks more tiles)
     const void *tensor_map;  // CUtensorMap in device-visible memory, or null
     int *error_flag;
@@ -117,6 +118,9 @@ struct ResidentLaunch {
 
 // cudaErrorCooperativeLaunchTooLarge (and nothing launched) when the blocks
 // cannot all be resident at once.
+// Targets a pass from which the direct kernel queues a warp's unlike copies.
+constexpr int kDirectCompactFrom = 1 << 20;
+
 cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream);
 // The same MCS in one thread-block cluster holding a small plane in shared
 // memory; cudaErrorNotSupported (nothing launched) when it does not fit one.
