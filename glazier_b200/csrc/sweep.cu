@@ -367,6 +367,49 @@ __device__ __noinline__ void commit_moments(const SweepLaunch &a, uint32_t old, 
     }
 }
 
+// The volume and surface parts of a copy's energy change, added to `delta`
+// in a fixed order (old cell's volume, new cell's volume, old cell's
+// surface, new cell's surface), correctly rounded f32 throughout so a host
+// replay gets the same bits; the medium (label 0) has neither term.
+//   volume:  lambda ((v -/+ 1 - V_t)^2 - (v - V_t)^2) = lambda (1 -/+ 2 (v - V_t))
+//   surface: lambda ((s + ds - S_t)^2 - (s - S_t)^2) = lambda ds (2 (s - S_t) + ds)
+template <bool UNIFORM>
+__device__ __forceinline__ float size_terms(const SweepLaunch &a, uint32_t old, uint32_t nw, int t_old, int t_new,
+                                            int vol_old, int vol_new, int surf_old, int surf_new, int ds_old,
+                                            int ds_new, float delta) {
+    if (old != 0) {
+        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_old];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)vol_old, UNIFORM ? a.u_target_volume : a.t.target_volume[t_old]);
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, e))));
+        }
+    }
+    if (nw != 0) {
+        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_new];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)vol_new, UNIFORM ? a.u_target_volume : a.t.target_volume[t_new]);
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fadd_rn(__fmul_rn(2.0f, e), 1.0f)));
+        }
+    }
+    if (old != 0) {
+        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_old];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)surf_old, UNIFORM ? a.u_target_surface : a.t.target_surface[t_old]);
+            const float d = (float)ds_old;
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(d, __fadd_rn(__fmul_rn(2.0f, e), d))));
+        }
+    }
+    if (nw != 0) {
+        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_new];
+        if (lam != 0.0f) {
+            const float e = __fsub_rn((float)surf_new, UNIFORM ? a.u_target_surface : a.t.target_surface[t_new]);
+            const float d = (float)ds_new;
+            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(d, __fadd_rn(__fmul_rn(2.0f, e), d))));
+        }
+    }
+    return delta;
+}
+
 // Price one copy attempt whose neighbour pick is known to carry another label
 // and commit it if the Metropolis test takes it. UNIFORM: every label carries
 // one type, so the contact sum is J times a difference of like-neighbour
@@ -460,38 +503,7 @@ __device__ __forceinline__ void price_and_commit(const SweepLaunch &a, const int
         vol_new = base_new.x + dv;
         surf_new = base_new.y + ds;
     }
-    // lambda ((v -/+ 1 - V_t)^2 - (v - V_t)^2) = lambda (1 -/+ 2 (v - V_t))
-    if (old != 0) {
-        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_old];
-        if (lam != 0.0f) {
-            const float dv = __fsub_rn((float)vol_old, UNIFORM ? a.u_target_volume : a.t.target_volume[t_old]);
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, dv))));
-        }
-    }
-    if (nw != 0) {
-        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_new];
-        if (lam != 0.0f) {
-            const float dv = __fsub_rn((float)vol_new, UNIFORM ? a.u_target_volume : a.t.target_volume[t_new]);
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fadd_rn(__fmul_rn(2.0f, dv), 1.0f)));
-        }
-    }
-    // lambda ((s + ds - S_t)^2 - (s - S_t)^2) = lambda ds (2 (s - S_t) + ds)
-    if (old != 0) {
-        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_old];
-        if (lam != 0.0f) {
-            const float e = __fsub_rn((float)surf_old, UNIFORM ? a.u_target_surface : a.t.target_surface[t_old]);
-            const float dsf = (float)ds_old;
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
-        }
-    }
-    if (nw != 0) {
-        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_new];
-        if (lam != 0.0f) {
-            const float e = __fsub_rn((float)surf_new, UNIFORM ? a.u_target_surface : a.t.target_surface[t_new]);
-            const float dsf = (float)ds_new;
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(dsf, __fadd_rn(__fmul_rn(2.0f, e), dsf))));
-        }
-    }
+    delta = size_terms<UNIFORM>(a, old, nw, t_old, t_new, vol_old, vol_new, surf_old, surf_new, ds_old, ds_new, delta);
     if (EXTRAS && (a.has_length || a.has_chemotaxis || a.has_external || a.has_motility || a.has_nematic))
         delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
 
@@ -1242,36 +1254,7 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access
     const int vol_old = base_old.x + dv, surf_old = base_old.y + ds;
     unpack_delta(prev_new, dv, ds);
     const int vol_new = base_new.x + dv, surf_new = base_new.y + ds;
-    if (old != 0) {
-        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_old];
-        if (lam != 0.0f) {
-            const float e = __fsub_rn((float)vol_old, UNIFORM ? a.u_target_volume : a.t.target_volume[t_old]);
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fsub_rn(1.0f, __fmul_rn(2.0f, e))));
-        }
-    }
-    if (nw != 0) {
-        const float lam = UNIFORM ? a.u_lambda_volume : a.t.lambda_volume[t_new];
-        if (lam != 0.0f) {
-            const float e = __fsub_rn((float)vol_new, UNIFORM ? a.u_target_volume : a.t.target_volume[t_new]);
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fadd_rn(__fmul_rn(2.0f, e), 1.0f)));
-        }
-    }
-    if (old != 0) {
-        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_old];
-        if (lam != 0.0f) {
-            const float e = __fsub_rn((float)surf_old, UNIFORM ? a.u_target_surface : a.t.target_surface[t_old]);
-            const float d = (float)ds_old;
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(d, __fadd_rn(__fmul_rn(2.0f, e), d))));
-        }
-    }
-    if (nw != 0) {
-        const float lam = UNIFORM ? a.u_lambda_surface : a.t.lambda_surface[t_new];
-        if (lam != 0.0f) {
-            const float e = __fsub_rn((float)surf_new, UNIFORM ? a.u_target_surface : a.t.target_surface[t_new]);
-            const float d = (float)ds_new;
-            delta = __fadd_rn(delta, __fmul_rn(lam, __fmul_rn(d, __fadd_rn(__fmul_rn(2.0f, e), d))));
-        }
-    }
+    delta = size_terms<UNIFORM>(a, old, nw, t_old, t_new, vol_old, vol_new, surf_old, surf_new, ds_old, ds_new, delta);
     const float u = to_f32(draw(key_accept, target));
     if (!(delta <= 0.0f || u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
     acc.put(target, x, y, z, nw);
