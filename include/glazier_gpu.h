@@ -101,7 +101,8 @@ int glz_gpu_set_labels(glz_gpu *h, const uint32_t *labels, size_t sites);
 
 /* glz_gpu_set_labels from device memory of the handle's device (uint32 per
  * site): the zero-copy restart for a solver that keeps the lattice on the
- * device. The caller's writes to `labels` must be complete before the call
+ * device. No reference counterpart: the reference restarts from host labels
+ * only (Simulation::from_labels, glazier-core/src/cpu.rs:151-175). The caller's writes to `labels` must be complete before the call
  * (its stream synchronized, or the handle's stream made to wait on it); the
  * copy and the recount run on the handle's stream and are done when the call
  * returns. Memory of another device or of the host: GLZ_INVALID. */
@@ -151,7 +152,8 @@ int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len);
 
 /* glz_gpu_set_nematic_field from device memory: 2 f32 per site (q_xx, q_xy),
  * with the same checks, recount and ordering rule as
- * glz_gpu_set_labels_device. The host form rounds its f64 values to f32, so
+ * glz_gpu_set_labels_device. The device form of set_nematic_field
+ * (glazier-cuda/src/lib.rs:1199-1221), which takes host f64 pairs. The host form rounds its f64 values to f32, so
  * equal f32 values make the same run. */
 int glz_gpu_set_nematic_field_device(glz_gpu *h, const float *field, size_t len);
 
