@@ -126,6 +126,8 @@ def lib():
     L.glz_gpu_mcs.argtypes = [_P]
     L.glz_gpu_n_labels.restype = C.c_size_t
     L.glz_gpu_n_labels.argtypes = [_P]
+    L.glz_gpu_sweep_kernel.restype = C.c_char_p
+    L.glz_gpu_sweep_kernel.argtypes = [_P]
     L.glz_gpu_stream.restype = _P
     L.glz_gpu_stream.argtypes = [_P]
     L.glz_gpu_device_labels.restype = C.c_int

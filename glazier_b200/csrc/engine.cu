@@ -139,6 +139,7 @@ struct glz_gpu {
     bool compact = false; // ... queueing a warp's unlike copies (large passes)
     bool resident = false;  // ... with nothing between passes: every MCS in one launch
     bool cluster = false;   // ... a plane, in one thread-block cluster's shared memory
+    bool band = false;      // ... a large plane, streamed by row bands in one launch per call
     unsigned *barrier = nullptr;  // the resident sweep's grid barrier
     int max_ctas = 0;
     int uniform = -1;
@@ -544,7 +545,76 @@ int run_resident(glz_gpu *h, uint64_t steps, double *ms, bool *done) {
     return check_error_flag(h);
 }
 
+// The band sweep's step schedule: every MCS of the call in one launch when
+// nothing runs between steps, else one launch per MCS followed by the field
+// step (and the infection rule). Phases are bracketed by events when `ms` is
+// given. A plane the band sweep turns down goes back to the per-pass kernels.
+int run_steps(glz_gpu *h, uint64_t steps, double *ms);
+
+int run_band(glz_gpu *h, uint64_t steps, double *ms) {
+    const bool between = h->n_species > 0 || h->infect_species >= 0;
+    cudaEvent_t ev[3] = {};
+    if (ms) {
+        for (auto &e : ev) CU(cudaEventCreate(&e));
+        ms[0] = ms[1] = ms[2] = 0.0;
+    }
+    const auto done = [&](int rc) {
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        return rc;
+    };
+    while (steps > 0) {
+        // launches of at most 65536 MCS keep the barrier's arrival count
+        // (blocks x passes) far inside 32 bits
+        const uint64_t chunk = between ? 1 : (steps < 65536 ? steps : 65536);
+        glz::ResidentLaunch r{};
+        r.a = pass_launch(h, 0);
+        r.seed = h->seed;
+        r.step0 = (int32_t)h->mcs;
+        r.mcs = (int)chunk;
+        r.pass0 = (long long)h->pass_no;
+        for (int k = 0; k < 2; ++k) r.vs_base[k] = h->t.vs_base[k];
+        for (int k = 0; k < 3; ++k) r.vs_delta[k] = h->t.vs_delta[k];
+        r.barrier = h->barrier;
+        if (cudaMemsetAsync(h->barrier, 0, 2 * sizeof(unsigned), h->stream) != cudaSuccess)
+            return done(fail(GLZ_DRIVER, "barrier reset failed"));
+        if (ms && cudaEventRecord(ev[0], h->stream) != cudaSuccess) return done(fail(GLZ_DRIVER, "event record failed"));
+        const cudaError_t e = glz::launch_band_sweep(r, h->stream);
+        if (e == cudaErrorNotSupported) {
+            cudaGetLastError();
+            h->band = false;  // and later calls: the per-pass kernels take this plane
+            done(GLZ_OK);
+            return run_steps(h, steps, ms);
+        }
+        if (e != cudaSuccess) return done(fail(GLZ_DRIVER, std::string("band sweep: ") + cudaGetErrorString(e)));
+        h->pass_no += chunk * (uint64_t)h->g.ncol;
+        h->mcs += chunk;
+        if (ms && cudaEventRecord(ev[1], h->stream) != cudaSuccess) return done(fail(GLZ_DRIVER, "event record failed"));
+        if (h->n_species > 0)
+            if (int rc = field_step(h)) return done(rc);
+        if (h->infect_species >= 0) {
+            const cudaError_t ei = glz::launch_infection(h->cell_type, h->dose, (int)h->n_labels, h->infect_from,
+                                                         h->infect_to, h->infect_threshold, h->stream);
+            if (ei != cudaSuccess) return done(fail(GLZ_DRIVER, std::string("infection: ") + cudaGetErrorString(ei)));
+        }
+        if (ms) {
+            if (cudaEventRecord(ev[2], h->stream) != cudaSuccess || cudaEventSynchronize(ev[2]) != cudaSuccess)
+                return done(fail(GLZ_DRIVER, "event record failed"));
+            float t0 = 0.0f, t1 = 0.0f;
+            cudaEventElapsedTime(&t0, ev[0], ev[1]);
+            cudaEventElapsedTime(&t1, ev[1], ev[2]);
+            ms[0] += t0;
+            ms[1] += t1;
+        }
+        steps -= chunk;
+    }
+    done(GLZ_OK);
+    CU(cudaStreamSynchronize(h->stream));
+    return check_error_flag(h);
+}
+
 int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
+    if (h->band) return run_band(h, steps, ms);
     // resident launches of at most 65536 MCS, so the barrier's arrival count
     // (blocks x passes) stays far inside 32 bits
     double total[3] = {0.0, 0.0, 0.0};
@@ -767,6 +837,15 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     // (GLAZIER_SWEEP_CLUSTER=0: the cooperative grid instead).
     const char *cluster_env = std::getenv("GLAZIER_SWEEP_CLUSTER");
     h->cluster = h->resident && g.dim == 2 && !(cluster_env && cluster_env[0] == '0');
+    // A lean plane past the direct kernel's size streams its rows by bands in
+    // one launch per call when its rows are whole 16-byte units and a ring of
+    // them fits in shared memory (GLAZIER_SWEEP_BAND=0: never, =1: any lean
+    // plane it fits, small ones included).
+    const char *band_env = std::getenv("GLAZIER_SWEEP_BAND");
+    const int band_mode = band_env ? (band_env[0] == '0' ? 0 : 1) : -1;
+    h->band = h->lean && g.dim == 2 && band_mode != 0 && (band_mode == 1 || sites > direct_most) &&
+              glz::band_sweep_fits(w, hh);
+    if (h->band) h->direct = h->resident = h->cluster = false;
     h->host_tv = tv;
     h->host_lv = lv;
     h->host_ts = ts;
@@ -1025,6 +1104,16 @@ int glz_gpu_set_nematic_field_device(glz_gpu *h, const float *field, size_t len)
 uint64_t glz_gpu_mcs(const glz_gpu *h) { return h ? h->mcs : 0; }
 
 size_t glz_gpu_n_labels(const glz_gpu *h) { return h ? h->n_labels : 0; }
+
+const char *glz_gpu_sweep_kernel(const glz_gpu *h) {
+    if (!h) return "";
+    if (h->band) return "band";
+    if (!h->lean) return "general";
+    if (h->cluster) return "cluster";
+    if (h->resident) return "resident";
+    if (h->direct) return h->compact ? "compact" : "direct";
+    return "lean";
+}
 
 void *glz_gpu_stream(glz_gpu *h) { return h ? (void *)h->stream : nullptr; }
 

@@ -126,6 +126,15 @@ cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream);
 // memory; cudaErrorNotSupported (nothing launched) when it does not fit one.
 cudaError_t launch_cluster_sweep(const ResidentLaunch &r, cudaStream_t stream);
 
+// Every MCS of a call (or one MCS, when fields run between steps) of a large
+// lean plane in one cooperative launch: one CTA per SM streams its band of
+// rows through shared memory, a grid barrier between passes (band.cu).
+// cudaErrorNotSupported (nothing launched) when the plane does not suit it.
+cudaError_t launch_band_sweep(const ResidentLaunch &r, cudaStream_t stream);
+// Whether a plane of this width and height suits the band sweep on the
+// current device (rows whole 16-byte units, a ring of enough rows).
+bool band_sweep_fits(int w, int h);
+
 // Apply a motility pass's listed copies: the label, and the activity of a
 // type with a maximum (lib.rs:696-698); then clear the list.
 cudaError_t launch_apply_copies(const SweepLaunch &a, float *activity, cudaStream_t stream);

@@ -4,16 +4,17 @@
 // Some callers cannot call cudaMalloc: a host application that fixes its
 // device-memory budget at start-up and forbids allocation afterwards, or a
 // coupled solver that hands this library only buffers it owns. For them this
-// file keeps the field step's scratch (the intermediate sub-step fields and the
-// per-type secretion and uptake tables) in one file-scope __device__ array of
-// fixed size. Every GPU that loads the library holds that array until the
-// process exits.
+// file keeps the field step's scratch (a status word and the intermediate
+// sub-step fields) in one file-scope __device__ array of fixed size. Every GPU
+// that loads the library holds that array until the process exits. The
+// per-type secretion and uptake rates travel in the kernel's parameters.
 //
 // The arithmetic is the engine's field step (fields.cu): FTCS diffusion and
 // decay per sub-step, exchange folded into each species' last sub-step.
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -25,17 +26,22 @@
 
 namespace {
 
-constexpr int kTableFloats = 2 * glz::kMaxTypes * glz::kMaxSpecies;  // secretion then uptake
+constexpr int kStatusFloats = 64;                                     // one 256-byte line: the status word
 constexpr size_t kScratchFloats = (size_t)GLZ_NOALLOC_FIELD_SCRATCH;   // intermediate fields
+constexpr int kTable = glz::kMaxTypes * glz::kMaxSpecies;
 
-// The scratch: per-type tables first, then the intermediate sub-step fields.
-// In host code this name is a host-side stand-in, not a device address; the
+// The scratch: a status word (bit 0: a label at or past n_labels, bit 1: a
+// cell type at or past n_types), then the intermediate sub-step fields. In
+// host code this name is a host-side stand-in, not a device address; the
 // kernel is given the address cudaGetSymbolAddress returns for the current
 // device.
-static __device__ __align__(256) float g_noalloc_scratch[kTableFloats + kScratchFloats];
+static __device__ __align__(256) float g_noalloc_scratch[kStatusFloats + kScratchFloats];
 
+// The array's device address per device ordinal, looked up once per device
+// by the first call made with that device current. A context that
+// cudaDeviceReset replaces gets a new array; this cache does not follow it.
 constexpr int kMaxDevices = 64;
-float *g_scratch_ptr[kMaxDevices] = {};
+std::atomic<float *> g_scratch_ptr[kMaxDevices] = {};
 
 
 struct NoallocRound {
@@ -47,7 +53,8 @@ struct NoallocRound {
     const uint32_t *labels;
     const uint8_t *cell_type;
     uint32_t n_labels;
-    const float *secretion, *uptake;  // inside the scratch array
+    unsigned *status;  // the scratch's status word
+    float secretion[kTable], uptake[kTable];  // [type][species], n_types * n_species used
 };
 
 template <int DIM>
@@ -87,10 +94,19 @@ __global__ void __launch_bounds__(256) noalloc_round_kernel(const __grid_constan
         if (a.last[s]) {
             if (type < 0) {
                 const uint32_t l = a.labels[i];
-                // a label past the type table, or a type past the rate tables, takes
-                // no exchange rather than a read out of bounds
-                type = (l == 0 || l >= a.n_labels) ? 0x7fffffff : a.cell_type[l];
-                if (type >= a.n_types) type = 0x7fffffff;
+                // A label past the type table, or a type past the rate tables, is
+                // recorded in the status word (the call reports it) and takes no
+                // exchange rather than a read out of bounds.
+                if (l >= a.n_labels) {
+                    atomicOr(a.status, 1u);
+                    type = 0x7fffffff;
+                } else {
+                    type = l == 0 ? 0x7fffffff : a.cell_type[l];
+                    if (l != 0 && type >= a.n_types) {
+                        atomicOr(a.status, 2u);
+                        type = 0x7fffffff;
+                    }
+                }
             }
             if (type != 0x7fffffff) {
                 v = __fadd_rn(v, a.secretion[type * a.n_species + s]);
@@ -130,6 +146,14 @@ int glz_field_step_noalloc(int width, int height, int depth, int n_species, int 
     if (n_labels == 0) return fail(GLZ_INVALID, "the cell type table is empty");
     const long long sites = (long long)width * height * depth;
     if (sites >= (1LL << 31)) return fail(GLZ_INVALID, "the lattice has 2^31 sites or more");
+    {
+        // The stencil reads a site's neighbours while other threads write the
+        // output, so the two buffers may not share a byte.
+        const uintptr_t bytes = (uintptr_t)n_species * (uintptr_t)sites * sizeof(float);
+        const uintptr_t in0 = reinterpret_cast<uintptr_t>(fields_in), out0 = reinterpret_cast<uintptr_t>(fields_out);
+        if (in0 < out0 + bytes && out0 < in0 + bytes)
+            return fail(GLZ_INVALID, "fields_in and fields_out overlap; the step needs two distinct buffers");
+    }
     const int dim = depth > 1 ? 3 : 2;
     int rounds = 0, k[glz::kMaxSpecies];
     for (int s = 0; s < n_species; ++s) {
@@ -152,28 +176,23 @@ int glz_field_step_noalloc(int width, int height, int depth, int n_species, int 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail(GLZ_INVALID, "device ordinal past the 64 this entry point tracks");
-    if (!g_scratch_ptr[dev]) {
+    float *scratch = g_scratch_ptr[dev].load();
+    if (!scratch) {
         // Once per device, with that device current: the array's device
-        // address. The host symbol itself is not one.
+        // address. The host symbol itself is not one. Two threads that race
+        // here store the same address.
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<float *>(p);
+        scratch = static_cast<float *>(p);
+        g_scratch_ptr[dev].store(scratch);
     }
-    float *scratch = g_scratch_ptr[dev];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-
-    // The per-type tables go into the head of the scratch as f32, the type
-    // the engine's field step uses.
-    float tables[kTableFloats] = {};
-    const int cells = n_types * n_species;
-    for (int i = 0; i < cells; ++i) {
-        tables[i] = (float)secretion[i];
-        tables[glz::kMaxTypes * glz::kMaxSpecies + i] = (float)uptake[i];
-    }
-    e = cudaMemcpyAsync(scratch, tables, sizeof tables, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("table copy: ") + cudaGetErrorString(e));
-    float *fields = scratch + kTableFloats;
+    unsigned *status = reinterpret_cast<unsigned *>(scratch);
+    float *fields = scratch + kStatusFloats;
+    // The array keeps the last call's contents: the status word starts at zero.
+    e = cudaMemsetAsync(status, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("status reset: ") + cudaGetErrorString(e));
 
     const size_t n = (size_t)sites;
     int cur[glz::kMaxSpecies] = {};  // -1: the caller's input; 0/1: a scratch buffer
@@ -190,8 +209,12 @@ int glz_field_step_noalloc(int width, int height, int depth, int n_species, int 
         a.labels = labels;
         a.cell_type = cell_type;
         a.n_labels = (uint32_t)(n_labels > 0xffffffffu ? 0xffffffffu : n_labels);
-        a.secretion = scratch;
-        a.uptake = scratch + glz::kMaxTypes * glz::kMaxSpecies;
+        a.status = status;
+        // the rates as f32, the type the engine's field step uses
+        for (int c = 0; c < n_types * n_species; ++c) {
+            a.secretion[c] = (float)secretion[c];
+            a.uptake[c] = (float)uptake[c];
+        }
         for (int s = 0; s < n_species; ++s) {
             a.active[s] = r < k[s];
             a.last[s] = r == k[s] - 1;
@@ -211,6 +234,13 @@ int glz_field_step_noalloc(int width, int height, int depth, int n_species, int 
         for (int s = 0; s < n_species; ++s)
             if (a.active[s] && !a.last[s]) cur[s] = cur[s] < 0 ? 0 : 1 - cur[s];
     }
+    // Wait for the step, then report what the status word recorded.
+    unsigned flags = 0;
+    e = cudaMemcpyAsync(&flags, status, sizeof flags, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("field step: ") + cudaGetErrorString(e));
+    if (flags & 1u) return fail(GLZ_INVALID, "a label is not below the cell type count");
+    if (flags & 2u) return fail(GLZ_INVALID, "a cell type is not below the type count");
     return GLZ_OK;
 }
 

@@ -155,6 +155,12 @@ class GpuSimulation:
     def n_labels(self) -> int:
         return int(_lib.lib().glz_gpu_n_labels(self._h))
 
+    @property
+    def sweep_kernel(self) -> str:
+        """The sweep kernel the next step takes ("band", "lean", "direct",
+        "compact", "resident", "cluster" or "general")."""
+        return _lib.lib().glz_gpu_sweep_kernel(self._h).decode()
+
     def labels(self) -> np.ndarray:
         out = np.empty(self.sites, dtype=np.uint32)
         check(_lib.lib().glz_gpu_labels(self._h, ptr(out), out.size))

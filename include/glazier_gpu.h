@@ -164,6 +164,12 @@ uint64_t glz_gpu_mcs(const glz_gpu *h);
  * lib.rs:1365). */
 size_t glz_gpu_n_labels(const glz_gpu *h);
 
+/* The sweep kernel the handle's next step takes: "band", "lean", "direct",
+ * "compact", "resident", "cluster" or "general" (the engine picks it from
+ * the model's terms and the lattice's size). A diagnostic with no reference
+ * counterpart: the reference has one kernel (lib.rs:436-716). Never NULL. */
+const char *glz_gpu_sweep_kernel(const glz_gpu *h);
+
 /* The handle's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against the engine's. No reference counterpart: the
  * reference keeps its stream private (lib.rs:751). */
@@ -255,7 +261,7 @@ void *glz_adj_stream(glz_adj *h);
 void glz_adj_destroy(glz_adj *h);
 
 /* The most f32 values of intermediate fields glz_field_step_noalloc holds:
- * 4,194,304 (16 MiB), beside a table area of 1,024 values. */
+ * 4,194,304 (16 MiB), beside a 256-byte status line. */
 #define GLZ_NOALLOC_FIELD_SCRATCH (1u << 22)
 
 /*
@@ -267,25 +273,31 @@ void glz_adj_destroy(glz_adj *h);
  *
  * The arithmetic is the engine's own field step (glz_gpu_step's): per species
  * ceil(D / (1/(2 dim))) sub-steps of FTCS diffusion and decay, secretion and
- * uptake by each site's owner folded into the species' last sub-step.
+ * uptake by each site's owner folded into the species' last sub-step. The
+ * engine's infection rule (glz_gpu_set_infection) is not part of it: a caller
+ * that needs it keeps an engine handle.
  *   width, height, depth   the lattice; n_species 1..8, n_types 1..64
  *   diffusion, decay       host, n_species values each
  *   secretion, uptake      host, n_types * n_species values, [type][species]
  *   labels, cell_type      device: one label per site; n_labels types
  *   fields_in, fields_out  device, n_species * sites f32, species-major;
- *                          distinct buffers
+ *                          two buffers that share no byte (else GLZ_INVALID)
  *   stream                 a cudaStream_t, or NULL for the default stream
- * The work is queued on `stream`; the call does not wait for it.
+ * The work runs on `stream` and the call waits for it. A label at or past
+ * n_labels, or a cell type at or past n_types, gets diffusion and decay only
+ * and the call returns GLZ_INVALID with the reason, as glz_gpu_step does.
  *
- * The scratch (the per-type tables and up to GLZ_NOALLOC_FIELD_SCRATCH
- * values of intermediate fields: none for one sub-step, one buffer per
- * species for two, two for three or more) lives in one fixed array in device
- * memory that every GPU loading this library holds until the process exits. A
- * step needing more is refused with GLZ_INVALID. The first call on a device
- * looks up that array's device address; make it before any stream capture.
- * Every call shares the array and nothing in it needs to start at zero, but
- * two calls whose work overlaps on the GPU race on it: order them on one
- * stream or wait between them.
+ * The scratch (a status word and up to GLZ_NOALLOC_FIELD_SCRATCH values of
+ * intermediate fields: none for one sub-step, one buffer per species for
+ * two, two for three or more) lives in one fixed array in device memory that
+ * every GPU loading this library holds until the process exits; the rate
+ * tables travel in the kernel's parameters. A step needing more scratch is
+ * refused with GLZ_INVALID. The first call on a device looks up that array's
+ * device address and keeps it for the life of the process (a context that
+ * cudaDeviceReset replaces is not followed); make that first call before any
+ * stream capture. Every call shares the array, and each clears its status
+ * word first; two calls whose work overlaps on the GPU race on it: order them
+ * on one stream or wait between them.
  */
 int glz_field_step_noalloc(int width, int height, int depth, int n_species, int n_types, const double *diffusion,
                            const double *decay, const double *secretion, const double *uptake,

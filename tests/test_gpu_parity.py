@@ -190,21 +190,22 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("kernel", ["cluster", "resident", "direct", "compact", "lean", "general"])
+@pytest.mark.parametrize("kernel", ["band", "cluster", "resident", "direct", "compact", "lean", "general"])
 @pytest.mark.parametrize("ctas", ["0", "3"])
 @pytest.mark.parametrize("tma", ["1", "0"])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, kernel, monkeypatch):
     """`ctas` 3 caps the sweep's persistent grid at three CTAs, so every CTA
     walks several tiles and every window buffer takes tensor copies; `kernel`
-    forces the lean models onto the cluster (a plane held in one thread-block
+    forces the lean models onto the band sweep (a plane's rows streamed by
+    bands, every pass of a call in one launch), the cluster (a plane held in one thread-block
     cluster's shared memory), the resident (every MCS of a call in one
     launch, for models with nothing between passes), the direct (one thread a
     target, or with `compact` each warp's unlike copies queued and priced in
     full rounds), the lean or the general kernel (models with other terms
     always take the general one)."""
-    if kernel in ("cluster", "resident", "direct", "compact") and (tma == "0" or ctas == "3"):
-        pytest.skip("the resident and direct kernels stage nothing and have no persistent grid")
+    if kernel in ("band", "cluster", "resident", "direct", "compact") and (tma == "0" or ctas == "3"):
+        pytest.skip("the band, resident and direct kernels take no tensor copies and no grid cap")
     made, steps = CASES[name]()
     start, fields = made if isinstance(made, tuple) else (made, None)
     monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
@@ -214,6 +215,7 @@ def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, k
     monkeypatch.setenv("GLAZIER_SWEEP_COMPACT", "1" if kernel == "compact" else "0")
     monkeypatch.setenv("GLAZIER_SWEEP_RESIDENT", "1" if kernel in ("cluster", "resident") else "0")
     monkeypatch.setenv("GLAZIER_SWEEP_CLUSTER", "1" if kernel == "cluster" else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_BAND", "1" if kernel == "band" else "0")
     gpu = device.GpuSimulation.from_start(start, fields)
     replay = ReplayOracle.from_start(start, fields)
     for chunk in (1, steps - 1):
