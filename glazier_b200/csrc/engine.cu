@@ -816,7 +816,12 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     const char *direct_env = std::getenv("GLAZIER_SWEEP_DIRECT");
     const int direct_mode = direct_env ? (direct_env[0] == '0' ? 0 : 1) : -1;
     const long long direct_most = g.dim == 2 ? 1024LL * 1024LL : sites;
-    h->direct = h->lean && (direct_mode == 1 || (direct_mode == -1 && sites <= direct_most));
+    // Models with other terms (length, chemotaxis, connectivity, motility,
+    // drift, nematic, division and death) take the direct kernel on planes up
+    // to 1024^2 and volumes up to 128^3, where the tiled kernel's window
+    // staging costs more than it saves.
+    const long long direct_most_general = g.dim == 2 ? 1024LL * 1024LL : 128LL * 128LL * 128LL;
+    h->direct = direct_mode == 1 || (direct_mode == -1 && sites <= (h->lean ? direct_most : direct_most_general));
     // From a million targets a pass the direct kernel queues each warp's
     // unlike copies and prices them in full rounds (GLAZIER_SWEEP_COMPACT=1:
     // at any size, =0: never).
@@ -831,7 +836,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     // launch at any size or dimension.
     const char *resident_env = std::getenv("GLAZIER_SWEEP_RESIDENT");
     const int resident_mode = resident_env ? (resident_env[0] == '0' ? 0 : 1) : -1;
-    h->resident = h->direct && ns == 0 && !h->has_pop &&
+    h->resident = h->lean && h->direct && ns == 0 && !h->has_pop &&
                   (resident_mode == 1 || (resident_mode == -1 && g.dim == 2 && sites <= 512LL * 512LL));
     // A resident plane runs in one thread-block cluster when it fits one
     // (GLAZIER_SWEEP_CLUSTER=0: the cooperative grid instead).
@@ -1108,11 +1113,10 @@ size_t glz_gpu_n_labels(const glz_gpu *h) { return h ? h->n_labels : 0; }
 const char *glz_gpu_sweep_kernel(const glz_gpu *h) {
     if (!h) return "";
     if (h->band) return "band";
-    if (!h->lean) return "general";
     if (h->cluster) return "cluster";
     if (h->resident) return "resident";
     if (h->direct) return h->compact ? "compact" : "direct";
-    return "lean";
+    return h->lean ? "lean" : "general";
 }
 
 void *glz_gpu_stream(glz_gpu *h) { return h ? (void *)h->stream : nullptr; }

@@ -1145,11 +1145,24 @@ __device__ __forceinline__ void direct_site(const SweepLaunch &a, int colour, in
     z = DIM == 3 ? 2 * (j / (hw * hh)) + ((colour >> 2) & 1) : 0;
 }
 
+// The connectivity veto (lib.rs:511-521) for a direct pass: the ring
+// positions of `old` around target (x, y, z), read where they lie, must be
+// one piece.
+__device__ __noinline__ bool direct_ring_one_piece(const SweepLaunch &a, int x, int y, int z, uint32_t old) {
+    const int W = a.g.w, H = a.g.h, D = a.g.d;
+    uint32_t present = 0;
+    for (int k = 0; k < a.g.ring_n; ++k) {
+        const int nx = wrap(x + a.g.ring[k][0], W), ny = wrap(y + a.g.ring[k][1], H), nz = wrap(z + a.g.ring[k][2], D);
+        if (a.labels[((size_t)nz * H + ny) * W + nx] == old) present |= 1u << k;
+    }
+    return one_piece(present, a.g.adjacency);
+}
+
 // The copy attempt at target (x, y, z) of a direct pass, its labels and
 // tallies found through `acc`: a target's neighbours are other colours, which
 // no copy in the pass changes. Priced with price_and_commit's arithmetic
 // operation for operation.
-template <int DIM, int NOFF, bool UNIFORM, class Access>
+template <int DIM, int NOFF, bool UNIFORM, class Access, bool EXTRAS = false>
 __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access &acc, uint64_t key_pick,
                                               uint64_t key_accept, int x, int y, int z, int known_pick = -1) {
     const int W = a.g.w, H = a.g.h, D = a.g.d;
@@ -1201,6 +1214,8 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access
         }
     }
     if (old != 0 && like_old == 0 && !acc.keeps_other_colour(old)) return;
+    if (EXTRAS && old != 0 && a.g.ring_n > 0 && a.t.connected[t_old] && !direct_ring_one_piece(a, x, y, z, old))
+        return;
     const int ds_old = 2 * like_old - NOFF;
     const int ds_new = NOFF - 2 * like_new;
     int dv, ds;
@@ -1209,11 +1224,19 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access
     unpack_delta(prev_new, dv, ds);
     const int vol_new = base_new.x + dv, surf_new = base_new.y + ds;
     delta = size_terms<UNIFORM>(a, old, nw, t_old, t_new, vol_old, vol_new, surf_old, surf_new, ds_old, ds_new, delta);
+    if (EXTRAS && (a.has_length || a.has_chemotaxis || a.has_external || a.has_motility || a.has_nematic))
+        delta = extra_terms<DIM>(a, old, nw, t_old, t_new, vol_old, vol_new, x, y, z, pick, target, delta);
     const float u = to_f32(draw(key_accept, target));
     if (!(delta <= 0.0f || u < metropolis_exp(__fmul_rn(-delta, a.beta)))) return;
-    acc.put(target, x, y, z, nw);
+    if (EXTRAS && a.has_motility) {
+        const int k = atomicAdd(a.pending_count, 1);
+        a.pending[k] = make_uint2(target, nw);
+    } else {
+        acc.put(target, x, y, z, nw);
+    }
     if (old != 0) acc.tally(old, -1, ds_old);
     if (nw != 0) acc.tally(nw, 1, ds_new);
+    if (EXTRAS && a.tracks) commit_moments<DIM>(a, old, nw, x, y, z);
 }
 
 // The offset of neighbour `pick`, chosen among compile-time constants (the
@@ -1246,7 +1269,7 @@ __device__ __forceinline__ void pick_offset(int pick, int &dx, int &dy, int &dz)
 // grid hides more latency and is as fast or faster.
 constexpr int kDirectCompactK = 4;
 
-template <int DIM, int NOFF, bool UNIFORM, int K>
+template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
 __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant__ SweepLaunch a) {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
@@ -1258,7 +1281,7 @@ __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant
         if (j < targets) {
             int x, y, z;
             direct_site<DIM>(a, a.colour, j, x, y, z);
-            direct_target<DIM, NOFF, UNIFORM>(a, acc, v.key_pick, v.key_accept, x, y, z);
+            direct_target<DIM, NOFF, UNIFORM, GlobalPass, EXTRAS>(a, acc, v.key_pick, v.key_accept, x, y, z);
         }
     } else {
         __shared__ int queue[8][32 * K];
@@ -1294,7 +1317,8 @@ __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant
         for (int e = lane; e < total; e += 32) {
             int x, y, z;
             direct_site<DIM>(a, a.colour, queue[warp][e], x, y, z);
-            direct_target<DIM, NOFF, UNIFORM>(a, acc, v.key_pick, v.key_accept, x, y, z, picks[warp][e]);
+            direct_target<DIM, NOFF, UNIFORM, GlobalPass, EXTRAS>(a, acc, v.key_pick, v.key_accept, x, y, z,
+                                                                  picks[warp][e]);
         }
     }
     rotate_tallies<DIM>(a);
@@ -1656,11 +1680,15 @@ static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = programmatic_launch();
+    // a motility pass follows its predecessor's copy list and a memset, not a kernel
+    attr[0].val.programmaticStreamSerializationAllowed = programmatic_launch() && !a.has_motility;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK>, a)
-                   : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0>, a);
+    if (!a.lean)  // every term: length, chemotaxis, connectivity, motility, drift, nematic, moments
+        return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
+                       : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, true>, a);
+    return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
+                   : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, false>, a);
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
@@ -1711,8 +1739,8 @@ static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
         tmap = *static_cast<const CUtensorMap *>(a.tensor_map);
     else
         memset(&tmap, 0, sizeof tmap);
-    if (a.lean) return a.direct ? launch_direct<DIM, NOFF, UNIFORM>(a, stream)
-                                : launch_lean<DIM, NOFF, UNIFORM>(a, tmap, stream);
+    if (a.direct) return launch_direct<DIM, NOFF, UNIFORM>(a, stream);
+    if (a.lean) return launch_lean<DIM, NOFF, UNIFORM>(a, tmap, stream);
     using T = Tile<DIM>;
     static int grid_cap = 0;
     const size_t smem = sizeof(SweepSmem<DIM>) + 128;
