@@ -154,6 +154,19 @@ struct glz_gpu {
     int *error_flag = nullptr;
     unsigned long long *medium = nullptr;
 
+    // Population models keep the live label count on the device (divisions
+    // add to it there). The host holds an upper bound of it for the work it
+    // has queued, and after each population step the count is copied into a
+    // pinned slot and marked by an event, so the bound tightens without
+    // waiting for the stream whenever a copy has landed.
+    static constexpr int kCountSlots = 4;
+    int *n_live = nullptr;
+    int *n_seen = nullptr;  // pinned, kCountSlots entries
+    cudaEvent_t n_event[kCountSlots] = {};
+    uint64_t n_step[kCountSlots] = {};  // the population step each slot's copy follows
+    uint64_t pop_steps = 0;             // population steps queued
+    size_t n_bound = 0;
+
     // population scratch, `cap` entries each
     unsigned char *mode = nullptr;
     double *plan = nullptr;
@@ -286,12 +299,16 @@ int alloc_labels(glz_gpu *h, size_t cap) {
     return GLZ_OK;
 }
 
-int recount(glz_gpu *h) {
+// Recount every tally from the lattice; with `when` (a device flag) only if
+// it is nonzero when the recount runs.
+int recount(glz_gpu *h, const int *when = nullptr) {
     const uint64_t p = h->pass_no;
     glz::RecountLaunch r{};
     r.g = h->g;
     r.labels = h->labels;
-    r.n_labels = (int)h->n_labels;
+    r.n_labels = (int)(h->n_live ? h->cap : h->n_labels);
+    r.n_live = h->n_live;
+    r.when = when;
     r.vs_base = h->t.vs_base[p % 2];
     r.mom_base = h->t.mom_base[p % 2];
     for (int k = 0; k < 3; ++k) {
@@ -310,7 +327,25 @@ int recount(glz_gpu *h) {
 int settle(glz_gpu *h) {
     const uint64_t p = h->pass_no;
     CU(glz::launch_settle(h->t.vs_base[p % 2], h->t.vs_delta[(p + 2) % 3], h->t.mom_base[p % 2],
-                          h->t.mom_delta[(p + 2) % 3], h->g.nm, (int)h->n_labels, h->tracks, h->stream));
+                          h->t.mom_delta[(p + 2) % 3], h->g.nm, (int)(h->n_live ? h->cap : h->n_labels), h->tracks,
+                          h->n_live, h->stream));
+    return GLZ_OK;
+}
+
+// The exact live label count of a population model, read after the stream
+// drains; the types of labels born since the last read join the host copy.
+int sync_count(glz_gpu *h) {
+    if (!h->n_live) return GLZ_OK;
+    int n = 0;
+    CU(cudaMemcpyAsync(&n, h->n_live, sizeof n, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if ((size_t)n > h->n_labels) {
+        h->cell_type_host.resize((size_t)n);
+        CU(cudaMemcpy(h->cell_type_host.data() + h->n_labels, h->cell_type + h->n_labels, (size_t)n - h->n_labels,
+                      cudaMemcpyDeviceToHost));
+    }
+    h->n_labels = (size_t)n;
+    h->n_bound = (size_t)n;
     return GLZ_OK;
 }
 
@@ -366,6 +401,7 @@ glz::SweepLaunch pass_launch(glz_gpu *h, int colour) {
     a.vol_by_colour = h->t.vol_by_colour;
     a.anchor = h->t.anchor;
     a.n_labels = (int)h->n_labels;
+    a.n_live = h->n_live;
     a.uniform_type = h->uniform;
     a.uniform_contact_exact = h->uniform_exact;
     a.uniform_contact = h->uniform_j;
@@ -434,11 +470,35 @@ int field_step(glz_gpu *h) {
     return GLZ_OK;
 }
 
-// Keep room for every cell to divide once: the most one step can add.
+// Label capacity a population model grows to: this many times its count.
+// Each step at most doubles the count, so the host can queue about log2 of
+// this many steps before it must read the count back.
+constexpr size_t kCapacityFactor = 16;
+
+// Keep room for every live cell to divide in the next step, the most one
+// step can add. The bound comes from the newest count copy that has landed
+// (each step queued after it at most doubles it); only when that is not
+// enough does the host wait for the exact count, and grow when that is not.
 int ensure_capacity(glz_gpu *h) {
-    if (h->cap >= 2 * h->n_labels) return GLZ_OK;
+    if (2 * h->n_bound <= h->cap) return GLZ_OK;
+    for (int back = 0; back < glz_gpu::kCountSlots && (uint64_t)back < h->pop_steps; ++back) {
+        const int slot = (int)((h->pop_steps - 1 - (uint64_t)back) % glz_gpu::kCountSlots);
+        const cudaError_t q = cudaEventQuery(h->n_event[slot]);
+        if (q == cudaErrorNotReady) {
+            cudaGetLastError();
+            continue;
+        }
+        CU(q);
+        size_t bound = (size_t)h->n_seen[slot];
+        for (uint64_t k = h->n_step[slot] + 1; k < h->pop_steps && bound <= h->cap; ++k) bound *= 2;
+        if (bound < h->n_bound) h->n_bound = bound;
+        break;
+    }
+    if (2 * h->n_bound <= h->cap) return GLZ_OK;
+    if (int rc = sync_count(h)) return rc;
+    if (2 * h->n_labels <= h->cap) return GLZ_OK;
     if (int rc = settle(h)) return rc;
-    return alloc_labels(h, 4 * h->n_labels);
+    return alloc_labels(h, kCapacityFactor * h->n_labels + 64);
 }
 
 int population(glz_gpu *h) {
@@ -453,6 +513,7 @@ int population(glz_gpu *h) {
     a.cell_type_out = h->cell_type;
     a.n_labels = (int)h->n_labels;
     a.cap = (int)h->cap;
+    a.n_live = h->n_live;
     a.vs_base = h->t.vs_base[p % 2];
     a.mom_base = h->t.mom_base[p % 2];
     a.anchor = h->t.anchor;
@@ -462,21 +523,16 @@ int population(glz_gpu *h) {
     a.moved = h->moved;
     a.daughter = h->daughter;
     a.counters = h->counters;
+    // plan, count, decide (the count grows on the device), apply; a step
+    // without an event changes nothing and its recount returns at once
     CU(glz::launch_population_plan(a, h->stream));
-    int counters[2] = {0, 0};
-    CU(cudaMemcpyAsync(counters, h->counters, sizeof counters, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
-    if (!counters[1]) return GLZ_OK;
     CU(glz::launch_population_apply(a, h->stream));
-    const size_t born = (size_t)counters[0];
-    if (born) {
-        h->cell_type_host.resize(h->n_labels + born);
-        CU(cudaMemcpyAsync(h->cell_type_host.data() + h->n_labels, h->cell_type + h->n_labels, born,
-                           cudaMemcpyDeviceToHost, h->stream));
-        h->n_labels += born;
-    }
-    if (int rc = recount(h)) return rc;
-    CU(cudaStreamSynchronize(h->stream));
+    if (int rc = recount(h, h->counters + 1)) return rc;
+    const int slot = (int)(h->pop_steps % glz_gpu::kCountSlots);
+    CU(cudaMemcpyAsync(&h->n_seen[slot], h->n_live, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaEventRecord(h->n_event[slot], h->stream));
+    h->n_step[slot] = h->pop_steps++;
+    h->n_bound *= 2;
     return GLZ_OK;
 }
 
@@ -593,8 +649,8 @@ int run_band(glz_gpu *h, uint64_t steps, double *ms) {
         if (h->n_species > 0)
             if (int rc = field_step(h)) return done(rc);
         if (h->infect_species >= 0) {
-            const cudaError_t ei = glz::launch_infection(h->cell_type, h->dose, (int)h->n_labels, h->infect_from,
-                                                         h->infect_to, h->infect_threshold, h->stream);
+            const cudaError_t ei = glz::launch_infection(h->cell_type, h->dose, (int)(h->n_live ? h->cap : h->n_labels), h->infect_from,
+                                                         h->infect_to, h->infect_threshold, h->n_live, h->stream);
             if (ei != cudaSuccess) return done(fail(GLZ_DRIVER, std::string("infection: ") + cudaGetErrorString(ei)));
         }
         if (ms) {
@@ -649,8 +705,8 @@ int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
         if (ms) CU(cudaEventRecord(ev[1], h->stream));
         if (rc == GLZ_OK && h->n_species > 0) rc = field_step(h);
         if (rc == GLZ_OK && h->infect_species >= 0) {
-            const cudaError_t e = glz::launch_infection(h->cell_type, h->dose, (int)h->n_labels, h->infect_from,
-                                                        h->infect_to, h->infect_threshold, h->stream);
+            const cudaError_t e = glz::launch_infection(h->cell_type, h->dose, (int)(h->n_live ? h->cap : h->n_labels), h->infect_from,
+                                                        h->infect_to, h->infect_threshold, h->n_live, h->stream);
             if (e != cudaSuccess) rc = fail(GLZ_DRIVER, std::string("infection: ") + cudaGetErrorString(e));
         }
         if (ms) CU(cudaEventRecord(ev[2], h->stream));
@@ -671,6 +727,7 @@ int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
             if (e) cudaEventDestroy(e);
     if (rc != GLZ_OK) return rc;
     CU(cudaStreamSynchronize(h->stream));
+    if (int rc2 = sync_count(h)) return rc2;
     return check_error_flag(h);
 }
 
@@ -870,7 +927,18 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     h->cell_type_host.assign(cell_type, cell_type + n_labels);
     h->n_labels = n_labels;
     find_uniform_type(h, m->contact, nt);
-    if ((rc = alloc_labels(h, h->has_pop ? 2 * n_labels + 16 : n_labels))) return bail(rc);
+    if ((rc = alloc_labels(h, h->has_pop ? kCapacityFactor * n_labels + 64 : n_labels))) return bail(rc);
+    if (h->has_pop) {
+        const int n = (int)n_labels;
+        if ((rc = dev_alloc(&h->n_live, 1))) return bail(rc);
+        if (cudaMemcpy(h->n_live, &n, sizeof n, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaHostAlloc((void **)&h->n_seen, glz_gpu::kCountSlots * sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+            return bail(fail(GLZ_DRIVER, "label count set-up failed"));
+        for (auto &e : h->n_event)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+                return bail(fail(GLZ_DRIVER, "cannot create an event"));
+        h->n_bound = n_labels;
+    }
 
     if (ns > 0) {
         if ((rc = dev_alloc(&h->field_buf, (size_t)2 * ns * sites))) return bail(rc);
@@ -1145,6 +1213,10 @@ void glz_gpu_destroy(glz_gpu *h) {
     cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->barrier); cudaFree(h->counters);
     free_tallies(h->t);
     free_population(h);
+    cudaFree(h->n_live);
+    if (h->n_seen) cudaFreeHost(h->n_seen);
+    for (auto &e : h->n_event)
+        if (e) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

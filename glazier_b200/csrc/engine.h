@@ -76,6 +76,10 @@ struct SweepLaunch {
     int *vol_by_colour;
     const int *anchor;
     int n_labels;
+    // Population models keep their live label count in device memory (it
+    // changes on the device when cells divide); n_labels is then the
+    // capacity and kernels read the count here. Null otherwise.
+    const int *n_live;
     int uniform_type;  // the type of every label when they share one, else -1
     int uniform_contact_exact;  // J m is exact in f32 for every |m| <= n_off (see sweep.cu)
     float uniform_contact;      // J[type][type] when uniform
@@ -203,8 +207,10 @@ cudaError_t launch_field_round(const FieldLaunch &a, cudaStream_t stream);
 
 // A cell of type `from` whose dose has reached `threshold` (units of 2^-24)
 // turns to type `to`.
+// With `n_live` (device memory) the count is read there and n_labels is the
+// capacity.
 cudaError_t launch_infection(uint8_t *cell_type, const unsigned long long *dose, int n_labels, int from, int to,
-                             long long threshold, cudaStream_t stream);
+                             long long threshold, const int *n_live, cudaStream_t stream);
 
 // Fixed-point scale of the infection dose: an uptake amount u adds
 // rint(u * 2^24), so the sum is exact and its order does not matter.
@@ -226,13 +232,20 @@ struct RecountLaunch {
     int tracks;
     const float *nematic;  // with the nematic term: its sums follow the moments
     int *error_flag;  // set to 2 when a label is not below n_labels
+    // Population models: the live count in device memory (n_labels is then
+    // the capacity), and a device flag the recount runs only when nonzero
+    // (the population step's event flag). Null: n_labels, and always.
+    const int *n_live;
+    const int *when;
 };
 
 cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream);
 
 // Fold the pending deltas into the base: B[s] += D[pd]; D[pd] = 0.
+// With `n_live` (device memory) the count is read there and n_labels is the
+// capacity.
 cudaError_t launch_settle(int2 *vs_base, long long *vs_delta, long long *mom_base, long long *mom_delta, int nm,
-                          int n_labels, int tracks, cudaStream_t stream);
+                          int n_labels, int tracks, const int *n_live, cudaStream_t stream);
 
 // The medium's volume and unlike-bond surface, counted from the lattice
 // (the sweep keeps no tally for label 0).
@@ -245,8 +258,9 @@ struct PopulationLaunch {
     uint32_t *labels;
     const uint8_t *cell_type_in;
     uint8_t *cell_type_out;  // may alias cell_type_in
-    int n_labels;
+    int n_labels;            // unused: the count lives in n_live
     int cap;
+    int *n_live;             // the live label count; decide adds the daughters to it
     const int2 *vs_base;     // settled tallies
     const long long *mom_base;
     const int *anchor;
@@ -256,7 +270,7 @@ struct PopulationLaunch {
     double *plan;            // 6 per cell: centroid, axis
     int *moved;
     uint32_t *daughter;
-    int *counters;           // [0] daughters issued, [1] events
+    int *counters;           // [0] daughters issued, [1] events (the recount's `when`)
 };
 
 // Record the message glz_last_error() returns on this thread.

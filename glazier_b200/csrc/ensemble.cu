@@ -249,7 +249,7 @@ int run(glz_ens *h, uint64_t steps, bool graph, double *ms) {
 
 int settle_all(glz_ens *h) {
     const long long p = h->pass;
-    CU(glz::launch_settle(h->vs_base[p % 2], h->vs_delta[(p + 2) % 3], nullptr, nullptr, 0, (int)h->total_cells, 0,
+    CU(glz::launch_settle(h->vs_base[p % 2], h->vs_delta[(p + 2) % 3], nullptr, nullptr, 0, (int)h->total_cells, 0, nullptr,
                           h->stream));
     return GLZ_OK;
 }

@@ -109,15 +109,17 @@ __global__ void __launch_bounds__(256) field_round_kernel(const __grid_constant_
 }
 
 __global__ void infection_kernel(uint8_t *cell_type, const unsigned long long *dose, int n_labels, int from, int to,
-                                 long long threshold) {
+                                 long long threshold, const int *n_live) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l == 0 || l >= n_labels) return;
+    const int n = n_live ? *n_live : n_labels;
+    if (l == 0 || l >= n) return;
     if (cell_type[l] == from && (long long)dose[l] >= threshold) cell_type[l] = (uint8_t)to;
 }
 
 cudaError_t launch_infection(uint8_t *cell_type, const unsigned long long *dose, int n_labels, int from, int to,
-                             long long threshold, cudaStream_t stream) {
-    infection_kernel<<<(n_labels + 255) / 256, 256, 0, stream>>>(cell_type, dose, n_labels, from, to, threshold);
+                             long long threshold, const int *n_live, cudaStream_t stream) {
+    infection_kernel<<<(n_labels + 255) / 256, 256, 0, stream>>>(cell_type, dose, n_labels, from, to, threshold,
+                                                                 n_live);
     return cudaGetLastError();
 }
 

@@ -14,9 +14,12 @@
 //   decide  one CTA, in label order: a cut that moves nothing or everything
 //           is no division (cpu.rs:697-703); the rest take daughter labels
 //           n_labels, n_labels + 1, ... in their mothers' order, a prefix sum
-//           over the compacted list of dividing cells.
+//           over the compacted list of dividing cells. The live label count
+//           stays in device memory: decide reads it and adds the daughters,
+//           so no host read stands between steps.
 //   apply   per site: death to medium, the far side of a cut to the daughter.
-// The engine then recounts every tally from the lattice (cpu.rs:649-653).
+// The engine then recounts every tally from the lattice (cpu.rs:649-653),
+// a recount whose kernels return at once when decide found no event.
 
 #include "device.cuh"
 #include "engine.h"
@@ -36,7 +39,7 @@ __device__ __forceinline__ double along_cut(const Geometry &g, const int *anchor
 
 __global__ void plan_kernel(const __grid_constant__ PopulationLaunch a) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= a.n_labels) return;
+    if (l >= *a.n_live) return;
     a.moved[l] = 0;
     a.mode[l] = 0;
     if (l == 0) return;
@@ -115,15 +118,16 @@ __global__ void __launch_bounds__(1024) decide_kernel(const __grid_constant__ Po
     __shared__ int running;
     __shared__ int any_event;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int n_labels = *a.n_live;
     if (tid == 0) {
         running = 0;
         any_event = 0;
     }
     __syncthreads();
-    for (int base = 0; base < a.n_labels; base += blockDim.x) {
+    for (int base = 0; base < n_labels; base += blockDim.x) {
         const int l = base + tid;
         int keep = 0;
-        if (l < a.n_labels && l > 0) {
+        if (l < n_labels && l > 0) {
             const unsigned char m = a.mode[l];
             if (m == 1) {
                 const int moved = a.moved[l];
@@ -149,7 +153,7 @@ __global__ void __launch_bounds__(1024) decide_kernel(const __grid_constant__ Po
         __syncthreads();
         const int warp_before = wid == 0 ? 0 : warp_total[wid - 1];
         if (keep) {
-            const uint32_t d = (uint32_t)(a.n_labels + running + warp_before + before_in_warp);
+            const uint32_t d = (uint32_t)(n_labels + running + warp_before + before_in_warp);
             a.daughter[l] = d;
             a.cell_type_out[d] = a.cell_type_in[l];
         }
@@ -160,6 +164,7 @@ __global__ void __launch_bounds__(1024) decide_kernel(const __grid_constant__ Po
     if (tid == 0) {
         a.counters[0] = running;
         a.counters[1] = any_event;
+        *a.n_live = n_labels + running;  // every thread read the count before the first barrier
     }
 }
 
@@ -177,7 +182,7 @@ __global__ void apply_kernel(const __grid_constant__ PopulationLaunch a) {
 }
 
 cudaError_t launch_population_plan(const PopulationLaunch &a, cudaStream_t stream) {
-    plan_kernel<<<(a.n_labels + 255) / 256, 256, 0, stream>>>(a);
+    plan_kernel<<<(a.cap + 255) / 256, 256, 0, stream>>>(a);
     count_cut_kernel<<<(a.g.sites + 255) / 256, 256, 0, stream>>>(a);
     decide_kernel<<<1, 1024, 0, stream>>>(a);
     return cudaGetLastError();

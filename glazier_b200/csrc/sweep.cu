@@ -649,7 +649,8 @@ template <int DIM>
 __device__ __forceinline__ void rotate_tallies(const SweepLaunch &a) {
     const int NM = a.g.nm;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x; l < (size_t)a.n_labels; l += stride) {
+    const size_t n = a.n_live ? (size_t)*a.n_live : (size_t)a.n_labels;
+    for (size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += stride) {
         int dv, ds;
         unpack_delta(a.vs_prev[l], dv, ds);
         const int2 b = a.vs_base[l];

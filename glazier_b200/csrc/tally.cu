@@ -25,9 +25,34 @@ __device__ __forceinline__ void coords_of(const Geometry &g, size_t i, int &x, i
     z = (int)(row / h);
 }
 
-__global__ void fill_anchor_kernel(int *anchor, int n) {
+// The label count a recount covers: the live count in device memory for a
+// population model, else the launch's.
+__device__ __forceinline__ int recount_labels(const RecountLaunch &a) { return a.n_live ? *a.n_live : a.n_labels; }
+
+// Whether a conditional recount runs (the population step's event flag).
+__device__ __forceinline__ bool recount_runs(const RecountLaunch &a) { return !a.when || *a.when != 0; }
+
+// The tallies a recount rebuilds, zeroed for the live labels (a conditional
+// recount's stand-in for its memsets).
+__global__ void clear_tallies_kernel(const __grid_constant__ RecountLaunch a) {
+    if (!recount_runs(a)) return;
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= n) return;
+    if (l >= recount_labels(a)) return;
+    a.vs_base[l] = make_int2(0, 0);
+    for (int c = 0; c < a.g.ncol; ++c) a.vol_by_colour[(size_t)l * a.g.ncol + c] = 0;
+    for (int k = 0; k < 3; ++k) a.vs_delta[k][l] = 0;
+    if (a.tracks)
+        for (int j = 0; j < a.g.nm; ++j) {
+            a.mom_base[(size_t)l * a.g.nm + j] = 0;
+            for (int k = 0; k < 3; ++k) a.mom_delta[k][(size_t)l * a.g.nm + j] = 0;
+        }
+}
+
+__global__ void fill_anchor_kernel(const __grid_constant__ RecountLaunch a) {
+    if (!recount_runs(a)) return;
+    int *anchor = a.anchor;
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= recount_labels(a)) return;
     anchor[4 * l + 0] = 0;
     anchor[4 * l + 1] = 0;
     anchor[4 * l + 2] = 0;
@@ -68,6 +93,8 @@ __device__ __forceinline__ int unlike_neighbours(const Geometry &g, const uint32
 template <int DIM, int NOFF>
 __global__ void recount_counts_kernel(const __grid_constant__ RecountLaunch a) {
     constexpr uint32_t kNone = 0xffffffffu;
+    if (!recount_runs(a)) return;
+    const uint32_t n_labels = (uint32_t)recount_labels(a);
     const int W = a.g.w, H = a.g.h, D = a.g.d;
     const int lane = threadIdx.x & 31;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -76,7 +103,7 @@ __global__ void recount_counts_kernel(const __grid_constant__ RecountLaunch a) {
         const int y = row % H, z = row / H;
         const uint32_t i = (uint32_t)row * (uint32_t)W + (uint32_t)x;
         uint32_t l = x < W ? a.labels[i] : kNone;
-        if (l != kNone && l >= (uint32_t)a.n_labels) {
+        if (l != kNone && l >= n_labels) {
             atomicExch(a.error_flag, 2);
             l = kNone;
         }
@@ -149,8 +176,9 @@ static cudaError_t launch_counts_any(const RecountLaunch &a, cudaStream_t stream
 }
 
 __global__ void recount_anchor_kernel(const __grid_constant__ RecountLaunch a) {
+    if (!recount_runs(a)) return;
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= a.n_labels) return;
+    if (l >= recount_labels(a)) return;
     const int first = a.anchor[4 * l + 3];
     if (first == INT_MAX) return;
     int x, y, z;
@@ -161,10 +189,11 @@ __global__ void recount_anchor_kernel(const __grid_constant__ RecountLaunch a) {
 }
 
 __global__ void recount_moments_kernel(const __grid_constant__ RecountLaunch a) {
+    if (!recount_runs(a)) return;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)a.g.sites) return;
     const uint32_t l = a.labels[i];
-    if (l == 0 || l >= (uint32_t)a.n_labels) return;
+    if (l == 0 || l >= (uint32_t)recount_labels(a)) return;
     int x, y, z;
     coords_of(a.g, i, x, y, z);
     const int *an = &a.anchor[4 * (size_t)l];
@@ -197,20 +226,24 @@ __global__ void recount_moments_kernel(const __grid_constant__ RecountLaunch a) 
 }
 
 cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream) {
-    const size_t n = (size_t)a.n_labels;
-    cudaError_t e;
-    if ((e = cudaMemsetAsync(a.vs_base, 0, n * sizeof(int2), stream))) return e;
-    if ((e = cudaMemsetAsync(a.vol_by_colour, 0, n * a.g.ncol * sizeof(int), stream))) return e;
-    for (int k = 0; k < 3; ++k)
-        if ((e = cudaMemsetAsync(a.vs_delta[k], 0, n * sizeof(long long), stream))) return e;
-    if (a.tracks) {
-        if ((e = cudaMemsetAsync(a.mom_base, 0, n * a.g.nm * sizeof(long long), stream))) return e;
-        for (int k = 0; k < 3; ++k)
-            if ((e = cudaMemsetAsync(a.mom_delta[k], 0, n * a.g.nm * sizeof(long long), stream))) return e;
-    }
+    const size_t n = (size_t)a.n_labels;  // the count, or the capacity with n_live
     const int lb = (int)((n + 255) / 256);
     const int sb = (a.g.sites + 255) / 256;
-    fill_anchor_kernel<<<lb, 256, 0, stream>>>(a.anchor, (int)n);
+    if (a.n_live || a.when) {
+        clear_tallies_kernel<<<lb, 256, 0, stream>>>(a);
+    } else {
+        cudaError_t e;
+        if ((e = cudaMemsetAsync(a.vs_base, 0, n * sizeof(int2), stream))) return e;
+        if ((e = cudaMemsetAsync(a.vol_by_colour, 0, n * a.g.ncol * sizeof(int), stream))) return e;
+        for (int k = 0; k < 3; ++k)
+            if ((e = cudaMemsetAsync(a.vs_delta[k], 0, n * sizeof(long long), stream))) return e;
+        if (a.tracks) {
+            if ((e = cudaMemsetAsync(a.mom_base, 0, n * a.g.nm * sizeof(long long), stream))) return e;
+            for (int k = 0; k < 3; ++k)
+                if ((e = cudaMemsetAsync(a.mom_delta[k], 0, n * a.g.nm * sizeof(long long), stream))) return e;
+        }
+    }
+    fill_anchor_kernel<<<lb, 256, 0, stream>>>(a);
     if (cudaError_t e = launch_counts_any(a, stream)) return e;
     recount_anchor_kernel<<<lb, 256, 0, stream>>>(a);
     if (a.tracks) recount_moments_kernel<<<sb, 256, 0, stream>>>(a);
@@ -218,9 +251,9 @@ cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream) {
 }
 
 __global__ void settle_kernel(int2 *vs_base, long long *vs_delta, long long *mom_base, long long *mom_delta, int nm,
-                              int n, int tracks) {
+                              int n, int tracks, const int *n_live) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= n) return;
+    if (l >= (n_live ? *n_live : n)) return;
     int dv, ds;
     unpack_delta(vs_delta[l], dv, ds);
     int2 b = vs_base[l];
@@ -234,10 +267,10 @@ __global__ void settle_kernel(int2 *vs_base, long long *vs_delta, long long *mom
 }
 
 cudaError_t launch_settle(int2 *vs_base, long long *vs_delta, long long *mom_base, long long *mom_delta, int nm,
-                          int n_labels, int tracks, cudaStream_t stream) {
+                          int n_labels, int tracks, const int *n_live, cudaStream_t stream) {
     if (n_labels <= 0) return cudaSuccess;
     settle_kernel<<<(n_labels + 255) / 256, 256, 0, stream>>>(vs_base, vs_delta, mom_base, mom_delta, nm, n_labels,
-                                                              tracks);
+                                                              tracks, n_live);
     return cudaGetLastError();
 }
 
