@@ -134,18 +134,11 @@ def measured_peak() -> tuple:
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def committed_traffic():
-    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
-    path = ROOT / "profiles" / "lean_sweep_2d_4096.md"
-    if not path.exists():
-        return None
-    for line in path.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
+# DRAM bytes (read + write) of one launch of the headline sweep kernel on the
+# 4096^2 workload, from an ncu capture of that kernel (its summary is in
+# profiles/), with the kernel it was measured on. None until a capture of the
+# current kernel exists: a figure measured on another kernel is not reported.
+TRAFFIC = {"kernel": None, "bytes_per_launch": None}
 
 
 def ensemble_compare(mcs: int, device: int) -> dict:
@@ -610,7 +603,11 @@ def run_ours(args) -> None:
     total_ms = sweep_ms + field_ms + pop_ms
     slowest = max_over_ranks(total_ms)
     value = whole_job_rate(sites * args.steps, slowest / 1e3, world)
-    launches_per_step = 4  # four colour passes; the workload has no fields and no population
+    kernel = sim.sweep_kernel
+    # the band sweep runs a step's four colour passes in one launch; the
+    # per-pass kernels launch once per pass (the workload has no fields and no
+    # population, so nothing else runs)
+    launches_per_step = 1 if kernel == "band" else 4
 
     # end to end through the public API, host buffers pinned
     pinned_in = torch.from_numpy(start.labels.view(np.int32)).pin_memory()
@@ -631,11 +628,13 @@ def run_ours(args) -> None:
 
     peak, peak_kind = measured_peak()
     launch_s = (sweep_ms / 1e3) / (args.steps * launches_per_step)
-    bytes_per_launch = sites * BYTES_PER_SITE_UPDATE / 4
+    bytes_per_launch = sites * BYTES_PER_SITE_UPDATE / launches_per_step  # one MCS spread over its launches
     achieved = bytes_per_launch / launch_s / 1e9
+    kernel_name = {"band": "band_sweep_kernel<8,1> (one MCS: four colour passes)",
+                   "lean": "lean_sweep_kernel<2,8,1> (one colour pass)"}.get(kernel, kernel)
+    traffic = TRAFFIC["bytes_per_launch"] if TRAFFIC["kernel"] == kernel else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": committed_traffic(), "peak_source": peak_kind,
-                "kernel": "lean_sweep_kernel<2,8,1> (one colour pass)",
+                "traffic": traffic, "peak_source": peak_kind, "kernel": kernel_name,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3}
 
     sim.close()
@@ -654,17 +653,21 @@ def run_ours(args) -> None:
         "clocks": clocks.summary(),
         "phase_ms": {"sweep": sweep_ms, "fields": field_ms, "population": pop_ms},
     }
-    if world == 1 and not args.no_ensemble:
-        line["ensemble"] = ensemble_compare(100, torch.cuda.current_device())
-        line["mixed_ensemble"] = mixed_ensemble_compare(100, torch.cuda.current_device())
+    # The side legs, verbose ones first: a reader of the line's end (a log
+    # tail) sees the compact figures of the volume, infection, adjoint and
+    # ensemble legs and the CPU baseline.
+    dev_index = torch.cuda.current_device()
     if world == 1 and not args.no_published:
-        line["volume"] = volume_leg(20, torch.cuda.current_device(), peak)
-        line["published_rows"] = published_rows(torch.cuda.current_device())
-        line["coupling"] = coupling_leg(torch.cuda.current_device())
+        line["published_rows"] = published_rows(dev_index)
+        line["coupling"] = coupling_leg(dev_index)
+        line["volume"] = volume_leg(20, dev_index, peak)
     if world == 1 and not args.no_infection:
-        line["infection"] = infection_compare(200, 20, torch.cuda.current_device())
+        line["infection"] = infection_compare(200, 20, dev_index)
     if world == 1 and not args.no_adjoint:
-        line["adjoint"] = adjoint_compare(50, 10, 5, torch.cuda.current_device())
+        line["adjoint"] = adjoint_compare(50, 10, 5, dev_index)
+    if world == 1 and not args.no_ensemble:
+        line["ensemble"] = ensemble_compare(100, dev_index)
+        line["mixed_ensemble"] = mixed_ensemble_compare(100, dev_index)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size, args.cpu_seconds)
     print(json.dumps(line), flush=True)

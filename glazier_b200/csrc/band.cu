@@ -21,9 +21,14 @@
 //     expensive path runs with every lane busy. A row slot goes back to the
 //     producer when every consumer has finished the target rows that read it
 //     (an mbarrier per slot).
-//   - Passes are separated by a grid barrier (bounded, error flag 4): the
-//     per-cell tallies a pass reads are its snapshot, complete only once
-//     every band has finished the pass before.
+//   - The per-cell tallies a pass reads are its snapshot, complete only once
+//     every band has finished the pass before: a grid barrier (bounded, error
+//     flag 4) separates the passes' pricing. The labels a pass reads, though,
+//     changed in the pass before only on rows of that pass's parity, each in
+//     the band that priced it: a band's next rows are final once the band
+//     itself is done, except the one row at its edge that the neighbouring
+//     band owns, whose done flag the producer waits for. So a pass's rows
+//     stream in, and its light pass runs, while the grid barrier completes.
 
 #include <cuda_runtime.h>
 
@@ -43,6 +48,17 @@ constexpr long long kBandBarrierLimit = 1LL << 22;  // grid-barrier polls (each 
 #ifndef GLZ_BAND_WARPS
 #define GLZ_BAND_WARPS 16
 #endif
+// 1: a pass's rows start streaming as soon as the band (and, for its one
+// boundary row, the neighbouring band) has finished the pass before, and only
+// the pricing waits for the grid barrier; 0: every pass waits for the whole
+// grid before its first row.
+#ifndef GLZ_BAND_OVERLAP
+#define GLZ_BAND_OVERLAP 1
+#endif
+constexpr bool kBandOverlap = GLZ_BAND_OVERLAP != 0;
+// The barrier words: [0] arrivals, [1] barriers completed, then per CTA the
+// passes it has completed in this launch.
+constexpr int kBandMaxGrid = 1024;
 constexpr int kBandWarps = GLZ_BAND_WARPS;  // consumer warps; one more warp produces
 constexpr int kBandThreads = 32 * (kBandWarps + 1);
 constexpr int kBandConsumers = 32 * kBandWarps;
@@ -60,6 +76,7 @@ struct BandHead {
     float contact[kBandTypes * kBandTypes];
     int abort;   // a wait gave up: every warp stops at the pass's end
     int bar_ok;  // the grid barrier's outcome, for the whole block
+    unsigned epoch;  // passes of this launch the whole grid has completed, as this block has seen
 };
 
 __device__ __forceinline__ bool band_wait(unsigned long long *bar, uint32_t parity) {
@@ -72,6 +89,19 @@ __device__ __forceinline__ bool band_wait(unsigned long long *bar, uint32_t pari
             : "r"(b), "r"(parity)
             : "memory");
     return done != 0;
+}
+
+__device__ __forceinline__ unsigned band_load_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Wait (bounded) until the word at p reaches `want`: false if it gave up.
+__device__ __forceinline__ bool band_wait_word(const unsigned *p, unsigned want) {
+    for (long long spin = 0; spin < kBandBarrierLimit; ++spin)
+        if (band_load_acquire(p) >= want) return true;
+    return false;
 }
 
 // The neighbour offset of pick k, decoded from compile-time constants.
@@ -251,6 +281,7 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
             S.last[s] = 0;
         }
         S.abort = 0;
+        S.epoch = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     const bool small_types = a.n_types <= kBandTypes;
@@ -266,7 +297,9 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
         const int32_t step = (int32_t)((uint32_t)r.step0 + (uint32_t)m);
         for (int c = 0; c < 4; ++c) {
             const long long p = r.pass0 + (long long)m * 4 + c;
+            const unsigned k = (unsigned)(m * 4 + c);  // this launch's pass number
             const int cx = c & 1, cy = (c >> 1) & 1;
+            const int cy_before = ((c + 3) >> 1) & 1;  // the parity of the rows the pass before changed
             if (producer) {
                 if (lane == 0) {
                     // labels the previous pass wrote (generic proxy) are read by bulk copies (async proxy)
@@ -283,6 +316,20 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                         }
                         int yy = 2 * lo + cy - 1 + j;
                         yy += yy < 0 ? H : (yy >= H ? -H : 0);
+                        if (kBandOverlap && k > 0 && (yy & 1) == cy_before) {
+                            // A row the pass before changed, in another band: wait for that
+                            // band to finish the pass (its labels then are final).
+                            const int tr = (yy - cy_before) / 2;
+                            const int owner = (int)(((long long)(tr + 1) * gridDim.x - 1) / NT);
+                            if (owner != (int)blockIdx.x) {
+                                if (!band_wait_word(r.barrier + 2 + owner, k)) {
+                                    atomicExch(a.error_flag, 4);
+                                    S.abort = 1;
+                                    break;
+                                }
+                                asm volatile("fence.proxy.async.global;" ::: "memory");
+                            }
+                        }
                         const uint32_t *src = a.labels + (size_t)yy * W;
                         uint32_t *dst = ring + (size_t)slot * RW;
                         const uint32_t bar = smem_addr(&S.full[slot]);
@@ -311,8 +358,44 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                 const BandPass v{c, stream_key(r.seed, step, c, 1), r.vs_base[p % 2], r.vs_delta[(p + 2) % 3],
                                  reinterpret_cast<unsigned long long *>(r.vs_delta[p % 3])};
                 const uint64_t key_pick = stream_key(r.seed, step, c, 0);
-                // The tally rotation for the next pass, which no thread of this one reads.
-                {
+                // Before a warp prices anything in this pass, the whole grid must have
+                // finished the pass before (the tallies are its snapshot). Warp 0 polls
+                // the grid barrier and publishes what it saw in shared memory; the
+                // other warps wait on that. Then the warp does its share of the tally
+                // rotation for the next pass, which no thread of this one reads.
+                bool synced = false;
+                const auto sync_pass = [&]() -> bool {
+                    if (synced) return true;
+                    synced = true;
+                    bool ok = true;
+                    if (kBandOverlap && k > 0) {
+                        if (lane == 0) {
+                            if (warp == 0) {
+                                ok = band_wait_word(r.barrier + 1, k);
+                                if (ok)
+                                    asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(smem_addr(&S.epoch)), "r"(k)
+                                                 : "memory");
+                            } else {
+                                ok = false;
+                                for (long long spin = 0; spin < kBandBarrierLimit; ++spin) {
+                                    unsigned e;
+                                    asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(e) : "r"(smem_addr(&S.epoch))
+                                                 : "memory");
+                                    if (e >= k) {
+                                        ok = true;
+                                        break;
+                                    }
+                                    if (*(volatile int *)&S.abort) break;
+                                }
+                            }
+                            if (!ok) {
+                                atomicExch(a.error_flag, 4);
+                                S.abort = 1;
+                            }
+                        }
+                        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                    }
+                    if (!ok) return false;
                     int2 *next_base = r.vs_base[(p + 1) % 2];
                     long long *clear = r.vs_delta[(p + 1) % 3];
                     const size_t stride = (size_t)gridDim.x * kBandConsumers;
@@ -323,7 +406,9 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                         next_base[l] = make_int2(b.x + dv, b.y + ds);
                         clear[l] = 0;
                     }
-                }
+                    return true;
+                };
+                if (!kBandOverlap) sync_pass();
                 const auto row_of = [&](uint32_t q) { return ring + (size_t)(q % (uint32_t)slots) * RW + kBandPad; };
                 const auto ready = [&](uint32_t q) {
                     return band_wait(&S.full[q % (uint32_t)slots], (q / (uint32_t)slots) & 1u);
@@ -372,9 +457,14 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                     // the previous row goes in one last short round so its rows can
                     // be let go; fewer than 32 of this row's stay held.
                     int taken = 0;
+                    bool stop = false;
                     for (;;) {
                         const int left = total - taken;
                         if (left < 32 && taken >= held) break;
+                        if (!sync_pass()) {
+                            stop = true;
+                            break;
+                        }
                         const int e = taken + lane;
                         if (e < total) {
                             const bool before = e < held;
@@ -387,6 +477,10 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                         taken += left < 32 ? left : 32;
                     }
                     __syncwarp();
+                    if (stop) {
+                        failed = true;
+                        break;
+                    }
                     if (t > 0) {  // the previous target row (sequence q - 2) is done: its rows q - 3, q - 2
                         release(q - 3u);
                         release(q - 2u);
@@ -404,7 +498,7 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                     h0 = r0;
                     hp = rp;
                 }
-                if (n > 0 && !failed) {
+                if (n > 0 && !failed && (held == 0 || sync_pass())) {
                     if (lane < held) {
                         const uint32_t entry = queue[lane];
                         band_price<NOFF, UNIFORM>(a, v, S.contact, small_types, hm, h0, hp,
@@ -416,6 +510,7 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                     release(ql);
                     release(ql + 1u);
                 }
+                if (!failed) sync_pass();  // a band that priced nothing still takes its share of the rotation
                 // this pass's label writes are read by the next pass's bulk copies
                 asm volatile("fence.proxy.async.global;" ::: "memory");
             }
@@ -429,7 +524,19 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                 __syncthreads();
                 return;
             }
-            if (!band_barrier(r.barrier, kbar++, &S.bar_ok)) {
+            if (kBandOverlap) {
+                // Arrive without waiting: the band's pass is done (its flag, for the
+                // neighbours' boundary rows) and the grid barrier counts it.
+                if (tid == 0) {
+                    __threadfence();
+                    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(r.barrier + 2 + blockIdx.x), "r"(k + 1u)
+                                 : "memory");
+                    if (atomicAdd(&r.barrier[0], 1u) + 1u == gridDim.x * (k + 1u)) {
+                        __threadfence();
+                        atomicExch(&r.barrier[1], k + 1u);
+                    }
+                }
+            } else if (!band_barrier(r.barrier, kbar++, &S.bar_ok)) {
                 if (tid == 0) atomicExch(a.error_flag, 4);
                 return;
             }
@@ -474,7 +581,7 @@ static cudaError_t launch_band(const ResidentLaunch &r, cudaStream_t stream) {
     if (cudaError_t e =
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_sweep_kernel<NOFF, UNIFORM>, kBandThreads, smem))
         return e;
-    if (per_sm < 1) return cudaErrorNotSupported;
+    if (per_sm < 1 || sms > kBandMaxGrid) return cudaErrorNotSupported;
     void *args[] = {&b};
     return cudaLaunchCooperativeKernel((const void *)band_sweep_kernel<NOFF, UNIFORM>, dim3((unsigned)sms),
                                        dim3(kBandThreads), args, smem, stream);
