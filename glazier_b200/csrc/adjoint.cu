@@ -89,15 +89,18 @@ struct Species {
     const float *in;    // the sub-step's input
     float *out;         // its output (after the exchange in the last round); may be null
     float *keep;        // last round: where to keep the exchange input; may be null
-    float d, e;
     int active, last;
 };
 
+// The per-sub-step diffusion and decay of each species live in device
+// memory (`de`: d for every species, then e), like the rate tables, so a
+// captured sequence of rounds serves any parameters with the same sub-step
+// counts.
 struct ForwardRound {
     Grid g;
     int n_species;
     const uint8_t *owner;  // this step's owner types
-    const float *sec, *upt;
+    const float *sec, *upt, *de;
     Species sp[glz::kMaxSpecies];
 };
 
@@ -114,8 +117,8 @@ __global__ void __launch_bounds__(kThreads) forward_round(const __grid_constant_
         if (!p.active) continue;
         const float here = p.in[i];
         const float sum = face_sum(a.g, p.in, nb);
-        float v = __fsub_rn(__fadd_rn(here, __fmul_rn(p.d, __fsub_rn(sum, __fmul_rn(faces, here)))),
-                            __fmul_rn(p.e, here));
+        const float d = a.de[s], e = a.de[a.n_species + s];
+        float v = __fsub_rn(__fadd_rn(here, __fmul_rn(d, __fsub_rn(sum, __fmul_rn(faces, here)))), __fmul_rn(e, here));
         if (p.last) {
             if (p.keep) p.keep[i] = v;
             if (t < 0) t = a.owner[i];
@@ -162,7 +165,6 @@ struct Adjoint {
     const float *exch;  // last round: the exchange input
     const float *lam;   // the adjoint of the round's output (of the step's output in the last round)
     float *lam_in;      // the adjoint of the sub-step's input
-    float d, e;
     int active, last;
 };
 
@@ -170,7 +172,7 @@ struct BackwardRound {
     Grid g;
     int n_species, n_types, n_grads;
     const uint8_t *owner;
-    const float *sec, *upt;
+    const float *sec, *upt, *de;
     double *partial;
     Adjoint sp[glz::kMaxSpecies];
 };
@@ -240,8 +242,8 @@ __global__ void __launch_bounds__(kThreads) backward_round(const __grid_constant
                 } else {
                     ls = face_sum(a.g, p.lam, nb);
                 }
-                p.lam_in[i] =
-                    __fsub_rn(__fadd_rn(l, __fmul_rn(p.d, __fsub_rn(ls, __fmul_rn(faces, l)))), __fmul_rn(p.e, l));
+                const float d = a.de[s], e = a.de[S + s];
+                p.lam_in[i] = __fsub_rn(__fadd_rn(l, __fmul_rn(d, __fsub_rn(ls, __fmul_rn(faces, l)))), __fmul_rn(e, l));
                 const float here = p.u[i];
                 const float us = face_sum(a.g, p.u, nb);
                 gd += (double)__fmul_rn(l, __fsub_rn(us, __fmul_rn(faces, here)));
@@ -314,6 +316,8 @@ struct glz_adj {
     float *work[2] = {};       // step outputs between checkpoints
     float *lam[2] = {};        // the adjoint fields
     float *d_sec = nullptr, *d_upt = nullptr;
+    float *d_de = nullptr;      // per-sub-step d then e per species
+    float *final_out = nullptr; // n_species * sites: the forward's last step, copied to the caller
     double *partial = nullptr;  // kBlocks rows of n_grads
     double *d_grads = nullptr;  // n_grads: d, e per species, then sec, upt per (type, species)
     std::vector<double> params;
@@ -321,6 +325,11 @@ struct glz_adj {
     int kmax = 0;
     int seg_kmax = -1;          // the kmax `seg` was sized for
     bool forward_done = false;
+    // The forward and backward sequences as CUDA graphs, captured for the
+    // sub-step counts in `graph_k` and replayed for any parameters with them.
+    cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
+    std::vector<int> graph_k;
+    int bwd_cur[glz::kMaxSpecies] = {};  // after a backward: which lam buffer holds each species
 };
 
 namespace {
@@ -350,13 +359,18 @@ int set_params(glz_adj *h, const double *params) {
         h->k[s] = substeps(params[s], h->g.dim);
         h->kmax = h->k[s] > h->kmax ? h->k[s] : h->kmax;
     }
-    std::vector<float> sec(T * S), upt(T * S);
+    std::vector<float> sec(T * S), upt(T * S), de(2 * S);
     for (int i = 0; i < T * S; ++i) {
         sec[i] = (float)params[2 * S + i];
         upt[i] = (float)params[2 * S + T * S + i];
     }
+    for (int sp = 0; sp < S; ++sp) {
+        de[sp] = (float)(params[sp] / (double)h->k[sp]);
+        de[S + sp] = (float)(params[S + sp] / (double)h->k[sp]);
+    }
     CU(cudaMemcpyAsync(h->d_sec, sec.data(), sec.size() * 4, cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->d_upt, upt.data(), upt.size() * 4, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemcpyAsync(h->d_de, de.data(), de.size() * 4, cudaMemcpyHostToDevice, h->stream));
     // the host vectors must outlive the copies
     CU(cudaStreamSynchronize(h->stream));
     if (h->seg_kmax != h->kmax) {
@@ -369,9 +383,6 @@ int set_params(glz_adj *h, const double *params) {
     return GLZ_OK;
 }
 
-float d_of(const glz_adj *h, int s) { return (float)(h->params[s] / (double)h->k[s]); }
-float e_of(const glz_adj *h, int s) { return (float)(h->params[h->n_species + s] / (double)h->k[s]); }
-
 // One step forward of every species, owners of step t, from `in` to `out`
 // (n_species * sites each, distinct buffers).
 int step_forward(glz_adj *h, int t, const float *in, float *out) {
@@ -382,6 +393,7 @@ int step_forward(glz_adj *h, int t, const float *in, float *out) {
     a.owner = h->owner + (size_t)t * n;
     a.sec = h->d_sec;
     a.upt = h->d_upt;
+    a.de = h->d_de;
     const float *cur[glz::kMaxSpecies];
     for (int s = 0; s < h->n_species; ++s) cur[s] = in + (size_t)s * n;
     for (int r = 0; r < h->kmax; ++r) {
@@ -389,8 +401,6 @@ int step_forward(glz_adj *h, int t, const float *in, float *out) {
             Species &p = a.sp[s];
             p.active = r < h->k[s];
             p.last = r == h->k[s] - 1;
-            p.d = d_of(h, s);
-            p.e = e_of(h, s);
             p.in = cur[s];
             p.keep = nullptr;
             p.out = p.last ? out + (size_t)s * n : h->tmp[r & 1] + (size_t)s * n;
@@ -410,6 +420,7 @@ int recompute(glz_adj *h, int sg, int len) {
     a.n_species = h->n_species;
     a.sec = h->d_sec;
     a.upt = h->d_upt;
+    a.de = h->d_de;
     for (int local = 0; local < len; ++local) {
         a.owner = h->owner + (size_t)(sg * h->every + local) * h->g.sites;
         for (int r = 0; r < h->kmax; ++r) {
@@ -417,8 +428,6 @@ int recompute(glz_adj *h, int sg, int len) {
                 Species &p = a.sp[s];
                 p.active = r < h->k[s];
                 p.last = r == h->k[s] - 1;
-                p.d = d_of(h, s);
-                p.e = e_of(h, s);
                 if (!p.active) continue;
                 p.in = seg_state(h, sg, local, r, s);
                 if (p.last) {
@@ -433,6 +442,99 @@ int recompute(glz_adj *h, int sg, int len) {
         }
     }
     CU(cudaGetLastError());
+    return GLZ_OK;
+}
+
+void drop_graphs(glz_adj *h) {
+    if (h->fwd_exec) cudaGraphExecDestroy(h->fwd_exec);
+    if (h->bwd_exec) cudaGraphExecDestroy(h->bwd_exec);
+    h->fwd_exec = h->bwd_exec = nullptr;
+    h->graph_k.clear();
+}
+
+// Record what `body` queues on the handle's stream as a graph, instantiated
+// into *exec; the capture ends whatever the body returns.
+int capture(glz_adj *h, cudaGraphExec_t *exec, int (*body)(glz_adj *)) {
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body(h);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("adjoint capture: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(GLZ_DRIVER, std::string("adjoint graph: ") + cudaGetErrorString(ei));
+    return GLZ_OK;
+}
+
+// Every step forward from checkpoint 0: a step's output goes to the next
+// checkpoint, to the work buffer the step did not read, or (the last) to
+// final_out.
+int forward_sequence(glz_adj *h) {
+    const size_t n = field_floats(h);
+    const float *cur = h->ckpt;
+    for (int t = 0; t < h->steps; ++t) {
+        float *dst;
+        if (t == h->steps - 1)
+            dst = h->final_out;
+        else if ((t + 1) % h->every == 0)
+            dst = h->ckpt + (size_t)((t + 1) / h->every) * n;
+        else
+            dst = cur == h->work[0] ? h->work[1] : h->work[0];
+        if (int rc = step_forward(h, t, cur, dst)) return rc;
+        cur = dst;
+    }
+    return GLZ_OK;
+}
+
+// The backward from lam[0] (the loss gradient at the final fields), segment
+// by segment from the last: recompute the segment's sub-step states, then
+// its rounds backward; the per-block gradient rows summed at the end.
+int backward_sequence(glz_adj *h) {
+    const int S = h->n_species, T = h->n_types, G = n_grads(h);
+    const size_t sites = h->g.sites;
+    const int grid = blocks_for(h) < kBlocks ? blocks_for(h) : kBlocks;
+    CU(cudaMemsetAsync(h->partial, 0, (size_t)grid * G * 8, h->stream));
+    int cur[glz::kMaxSpecies] = {};  // which lam buffer holds each species' adjoint
+    BackwardRound a{};
+    a.g = h->g;
+    a.n_species = S;
+    a.n_types = T;
+    a.n_grads = G;
+    a.sec = h->d_sec;
+    a.upt = h->d_upt;
+    a.de = h->d_de;
+    a.partial = h->partial;
+    const size_t smem = (size_t)kWarps * 2 * T * sizeof(double);
+    const int nseg = (h->steps + h->every - 1) / h->every;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int t0 = sg * h->every, len = (t0 + h->every < h->steps ? t0 + h->every : h->steps) - t0;
+        if (int rc = recompute(h, sg, len)) return rc;
+        for (int local = len - 1; local >= 0; --local) {
+            a.owner = h->owner + (size_t)(t0 + local) * sites;
+            for (int r = h->kmax - 1; r >= 0; --r) {
+                for (int s = 0; s < S; ++s) {
+                    Adjoint &p = a.sp[s];
+                    p.active = r < h->k[s];
+                    p.last = r == h->k[s] - 1;
+                    if (!p.active) continue;
+                    p.u = seg_state(h, sg, local, r, s);
+                    p.exch = seg_state(h, sg, local, h->k[s], s);
+                    p.lam = h->lam[cur[s]] + (size_t)s * sites;
+                    p.lam_in = h->lam[1 - cur[s]] + (size_t)s * sites;
+                    cur[s] = 1 - cur[s];
+                }
+                backward_round<<<grid, kThreads, smem, h->stream>>>(a);
+            }
+        }
+        CU(cudaGetLastError());
+    }
+    reduce_partials<<<(G + 127) / 128, 128, 0, h->stream>>>(h->partial, grid, G, h->d_grads);
+    CU(cudaGetLastError());
+    for (int s = 0; s < S; ++s) h->bwd_cur[s] = cur[s];
     return GLZ_OK;
 }
 
@@ -473,6 +575,8 @@ int glz_adj_create(int width, int height, int depth, int n_species, int n_types,
         cudaMalloc(&h->lam[1], n * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&h->d_sec, (size_t)n_types * n_species * 4) != cudaSuccess ||
         cudaMalloc(&h->d_upt, (size_t)n_types * n_species * 4) != cudaSuccess ||
+        cudaMalloc(&h->d_de, (size_t)2 * n_species * 4) != cudaSuccess ||
+        cudaMalloc(&h->final_out, n * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&h->partial, (size_t)kBlocks * n_grads(h) * 8) != cudaSuccess ||
         cudaMalloc(&h->d_grads, (size_t)n_grads(h) * 8) != cudaSuccess)
         return bail(fail(GLZ_DRIVER, "adjoint allocation failed"));
@@ -499,22 +603,17 @@ int glz_adj_forward(glz_adj *h, const double *params, const float *fields0, floa
     if (fields0 == fields_final) return fail(GLZ_INVALID, "the initial and final fields share a buffer");
     h->forward_done = false;
     if (int rc = set_params(h, params)) return rc;
-    const size_t n = field_floats(h);
-    // checkpoint 0 is the start; a step's output goes to the next checkpoint,
-    // to the work buffer the step did not read, or (the last) to the caller
-    CU(cudaMemcpyAsync(h->ckpt, fields0, n * 4, cudaMemcpyDeviceToDevice, h->stream));
-    const float *cur = h->ckpt;
-    for (int t = 0; t < h->steps; ++t) {
-        float *dst;
-        if (t == h->steps - 1)
-            dst = fields_final;
-        else if ((t + 1) % h->every == 0)
-            dst = h->ckpt + (size_t)((t + 1) / h->every) * n;
-        else
-            dst = cur == h->work[0] ? h->work[1] : h->work[0];
-        if (int rc = step_forward(h, t, cur, dst)) return rc;
-        cur = dst;
+    // the graphs hold the sub-step structure (and the segment buffers sized
+    // for it): new sub-step counts take new graphs
+    if (h->graph_k != h->k) drop_graphs(h);
+    if (!h->fwd_exec) {
+        if (int rc = capture(h, &h->fwd_exec, forward_sequence)) return rc;
+        h->graph_k = h->k;
     }
+    const size_t n = field_floats(h);
+    CU(cudaMemcpyAsync(h->ckpt, fields0, n * 4, cudaMemcpyDeviceToDevice, h->stream));  // checkpoint 0
+    CU(cudaGraphLaunch(h->fwd_exec, h->stream));
+    CU(cudaMemcpyAsync(fields_final, h->final_out, n * 4, cudaMemcpyDeviceToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     h->forward_done = true;
     return GLZ_OK;
@@ -523,51 +622,15 @@ int glz_adj_forward(glz_adj *h, const double *params, const float *fields0, floa
 int glz_adj_backward(glz_adj *h, const float *grad_final, double *grad_params, float *grad_fields0) {
     if (!h || !grad_final || !grad_params) return fail(GLZ_INVALID, "null argument");
     if (!h->forward_done) return fail(GLZ_INVALID, "backward before forward");
-    const int S = h->n_species, T = h->n_types, G = n_grads(h);
+    const int S = h->n_species, G = n_grads(h);
     const size_t n = field_floats(h), sites = h->g.sites;
-    const int grid = blocks_for(h) < kBlocks ? blocks_for(h) : kBlocks;
-    CU(cudaMemsetAsync(h->partial, 0, (size_t)grid * G * 8, h->stream));
+    if (!h->bwd_exec)
+        if (int rc = capture(h, &h->bwd_exec, backward_sequence)) return rc;
     CU(cudaMemcpyAsync(h->lam[0], grad_final, n * 4, cudaMemcpyDeviceToDevice, h->stream));
-    int cur[glz::kMaxSpecies] = {};  // which lam buffer holds each species' adjoint
-    BackwardRound a{};
-    a.g = h->g;
-    a.n_species = S;
-    a.n_types = T;
-    a.n_grads = G;
-    a.sec = h->d_sec;
-    a.upt = h->d_upt;
-    a.partial = h->partial;
-    const size_t smem = (size_t)kWarps * 2 * T * sizeof(double);
-    const int nseg = (h->steps + h->every - 1) / h->every;
-    for (int sg = nseg - 1; sg >= 0; --sg) {
-        const int t0 = sg * h->every, len = (t0 + h->every < h->steps ? t0 + h->every : h->steps) - t0;
-        if (int rc = recompute(h, sg, len)) return rc;
-        for (int local = len - 1; local >= 0; --local) {
-            a.owner = h->owner + (size_t)(t0 + local) * sites;
-            for (int r = h->kmax - 1; r >= 0; --r) {
-                for (int s = 0; s < S; ++s) {
-                    Adjoint &p = a.sp[s];
-                    p.active = r < h->k[s];
-                    p.last = r == h->k[s] - 1;
-                    p.d = d_of(h, s);
-                    p.e = e_of(h, s);
-                    if (!p.active) continue;
-                    p.u = seg_state(h, sg, local, r, s);
-                    p.exch = seg_state(h, sg, local, h->k[s], s);
-                    p.lam = h->lam[cur[s]] + (size_t)s * sites;
-                    p.lam_in = h->lam[1 - cur[s]] + (size_t)s * sites;
-                    cur[s] = 1 - cur[s];
-                }
-                backward_round<<<grid, kThreads, smem, h->stream>>>(a);
-            }
-        }
-        CU(cudaGetLastError());
-    }
-    reduce_partials<<<(G + 127) / 128, 128, 0, h->stream>>>(h->partial, grid, G, h->d_grads);
-    CU(cudaGetLastError());
+    CU(cudaGraphLaunch(h->bwd_exec, h->stream));
     if (grad_fields0)
         for (int s = 0; s < S; ++s)
-            CU(cudaMemcpyAsync(grad_fields0 + (size_t)s * sites, h->lam[cur[s]] + (size_t)s * sites, sites * 4,
+            CU(cudaMemcpyAsync(grad_fields0 + (size_t)s * sites, h->lam[h->bwd_cur[s]] + (size_t)s * sites, sites * 4,
                                cudaMemcpyDeviceToDevice, h->stream));
     std::vector<double> g(G);
     CU(cudaMemcpyAsync(g.data(), h->d_grads, (size_t)G * 8, cudaMemcpyDeviceToHost, h->stream));
@@ -587,6 +650,9 @@ void *glz_adj_stream(glz_adj *h) { return h ? (void *)h->stream : nullptr; }
 void glz_adj_destroy(glz_adj *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_graphs(h);
+    cudaFree(h->d_de);
+    cudaFree(h->final_out);
     cudaFree(h->owner);
     cudaFree(h->ckpt);
     cudaFree(h->seg);
