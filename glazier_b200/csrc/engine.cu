@@ -166,6 +166,19 @@ struct glz_gpu {
     uint64_t n_step[kCountSlots] = {};  // the population step each slot's copy follows
     uint64_t pop_steps = 0;             // population steps queued
     size_t n_bound = 0;
+    // The most cells one step can add: cells at or past their division
+    // volume hold disjoint sites, so at most sites / (the least division
+    // volume, and at least 4 sites, cpu.rs:681) of them divide.
+    size_t born_most = 0;
+
+    // Steps of a direct-kernel engine replay from one captured graph: its
+    // kernels read the step, pass and field buffers from `clock`, so the
+    // same graph serves every step. GLAZIER_ENGINE_GRAPH=0 queues every
+    // launch from the host instead.
+    glz::EngineClock *clock = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    bool graph_on = true;
+    uint64_t records_from = 0;  // count records older than this step predate graph replays
 
     // population scratch, `cap` entries each
     unsigned char *mode = nullptr;
@@ -236,6 +249,11 @@ void free_population(glz_gpu *h) {
     h->daughter = nullptr;
 }
 
+void drop_step_graph(glz_gpu *h) {
+    if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+    h->step_exec = nullptr;
+}
+
 // Per-label arrays sized for `cap` labels. The settled tallies, anchors,
 // per-colour volumes and cell types of the first n_labels entries carry over
 // exactly, so growing never changes a run; every delta word starts at zero.
@@ -296,6 +314,7 @@ int alloc_labels(glz_gpu *h, size_t cap) {
     cudaFree(h->dose);
     h->dose = dose;
     h->cap = cap;
+    drop_step_graph(h);  // its kernels hold the old arrays
     return GLZ_OK;
 }
 
@@ -470,19 +489,30 @@ int field_step(glz_gpu *h) {
     return GLZ_OK;
 }
 
-// Label capacity a population model grows to: this many times its count.
-// Each step at most doubles the count, so the host can queue about log2 of
-// this many steps before it must read the count back.
-constexpr size_t kCapacityFactor = 16;
+// The most labels a population model can hold after one more step from a
+// count of n: each live cell divides at most once, and at most born_most
+// cells divide.
+size_t after_step(const glz_gpu *h, size_t n) { return n + (h->born_most < n ? h->born_most : n); }
 
-// Keep room for every live cell to divide in the next step, the most one
-// step can add. The bound comes from the newest count copy that has landed
-// (each step queued after it at most doubles it); only when that is not
-// enough does the host wait for the exact count, and grow when that is not.
+// The label capacity a population model grows to from a count of n: room
+// for at least 16 steps of the most divisions, or 16 times the count when
+// that is less.
+size_t capacity_for(const glz_gpu *h, size_t n) {
+    size_t room = 16 * h->born_most;
+    if (room > 16 * n) room = 16 * n;
+    if (room < n) room = n;
+    return n + room + 64;
+}
+
+// Keep room for the next step's divisions. The host's bound of the count
+// comes from the newest count copy that has landed (each step queued after
+// it adds at most its most divisions); only when that is not enough does the
+// host wait for the exact count, and grow when that is not.
 int ensure_capacity(glz_gpu *h) {
-    if (2 * h->n_bound <= h->cap) return GLZ_OK;
+    if (after_step(h, h->n_bound) <= h->cap) return GLZ_OK;
     for (int back = 0; back < glz_gpu::kCountSlots && (uint64_t)back < h->pop_steps; ++back) {
         const int slot = (int)((h->pop_steps - 1 - (uint64_t)back) % glz_gpu::kCountSlots);
+        if (h->n_step[slot] < h->records_from) break;
         const cudaError_t q = cudaEventQuery(h->n_event[slot]);
         if (q == cudaErrorNotReady) {
             cudaGetLastError();
@@ -490,20 +520,27 @@ int ensure_capacity(glz_gpu *h) {
         }
         CU(q);
         size_t bound = (size_t)h->n_seen[slot];
-        for (uint64_t k = h->n_step[slot] + 1; k < h->pop_steps && bound <= h->cap; ++k) bound *= 2;
+        for (uint64_t k = h->n_step[slot] + 1; k < h->pop_steps && bound <= h->cap; ++k) bound = after_step(h, bound);
         if (bound < h->n_bound) h->n_bound = bound;
         break;
     }
-    if (2 * h->n_bound <= h->cap) return GLZ_OK;
+    if (after_step(h, h->n_bound) <= h->cap) return GLZ_OK;
     if (int rc = sync_count(h)) return rc;
-    if (2 * h->n_labels <= h->cap) return GLZ_OK;
+    if (after_step(h, h->n_labels) <= h->cap) return GLZ_OK;
     if (int rc = settle(h)) return rc;
-    return alloc_labels(h, kCapacityFactor * h->n_labels + 64);
+    return alloc_labels(h, capacity_for(h, h->n_labels));
 }
 
-int population(glz_gpu *h) {
-    if (int rc = ensure_capacity(h)) return rc;
-    if (int rc = settle(h)) return rc;
+// The population step's launches; `clocked` for a captured step (the settle
+// slots and the death draws' step from the clock).
+int population_launches(glz_gpu *h, bool clocked) {
+    if (clocked)
+        CU(glz::launch_settle_clocked(h->t, h->g.nm, (int)h->cap, h->tracks, h->n_live, h->clock, h->g.ncol,
+                                      h->stream));
+    else if (int rc = settle(h))
+        return rc;
+    // The pass count at the step's end has the parity of its start (ncol is
+    // even), so the base slot below is the same for every step of a graph.
     const uint64_t p = h->pass_no;
     glz::PopulationLaunch a{};
     a.g = h->g;
@@ -523,16 +560,23 @@ int population(glz_gpu *h) {
     a.moved = h->moved;
     a.daughter = h->daughter;
     a.counters = h->counters;
+    a.clock = clocked ? h->clock : nullptr;
+    a.seed = h->seed;
     // plan, count, decide (the count grows on the device), apply; a step
     // without an event changes nothing and its recount returns at once
     CU(glz::launch_population_plan(a, h->stream));
     CU(glz::launch_population_apply(a, h->stream));
-    if (int rc = recount(h, h->counters + 1)) return rc;
+    return recount(h, h->counters + 1);
+}
+
+int population(glz_gpu *h) {
+    if (int rc = ensure_capacity(h)) return rc;
+    if (int rc = population_launches(h, false)) return rc;
     const int slot = (int)(h->pop_steps % glz_gpu::kCountSlots);
     CU(cudaMemcpyAsync(&h->n_seen[slot], h->n_live, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(cudaEventRecord(h->n_event[slot], h->stream));
     h->n_step[slot] = h->pop_steps++;
-    h->n_bound *= 2;
+    h->n_bound = after_step(h, h->n_bound);
     return GLZ_OK;
 }
 
@@ -598,6 +642,98 @@ int run_resident(glz_gpu *h, uint64_t steps, double *ms, bool *done) {
     h->mcs += steps;
     *done = true;
     CU(cudaStreamSynchronize(h->stream));
+    return check_error_flag(h);
+}
+
+// One step with clocked launches, for capture: the direct passes (and the
+// motility copies), the activity decay, the field rounds, the infection rule,
+// the population step, then the clock's advance. Host state is left as it is.
+int queue_clocked_step(glz_gpu *h) {
+    for (int c = 0; c < h->g.ncol; ++c) {
+        glz::SweepLaunch a = pass_launch(h, c);
+        a.clock = h->clock;
+        a.seed = h->seed;
+        a.tal = h->t;
+        a.field_buf = h->field_buf;
+        CU(glz::launch_sweep(a, h->stream));
+        if (h->has_motility) CU(glz::launch_apply_copies(a, h->activity, h->stream));
+    }
+    if (h->has_motility) CU(glz::launch_activity_decay(h->activity, h->g.sites, h->stream));
+    int rounds = 0;
+    for (int s = 0; s < h->n_species; ++s) rounds = h->substeps[s] > rounds ? h->substeps[s] : rounds;
+    for (int r = 0; r < rounds; ++r) {
+        glz::FieldLaunch f{};
+        f.g = h->g;
+        f.n_species = h->n_species;
+        f.round = r;
+        f.labels = h->labels;
+        f.cell_type = h->cell_type;
+        f.secretion = h->sec;
+        f.uptake = h->upt;
+        f.infect_species = h->infect_species;
+        f.infect_from = h->infect_from;
+        f.dose = h->dose;
+        f.clock = h->clock;
+        f.field_buf = h->field_buf;
+        for (int s = 0; s < h->n_species; ++s) {
+            f.active[s] = r < h->substeps[s];
+            f.last[s] = r == h->substeps[s] - 1;
+            f.d[s] = h->fd[s];
+            f.decay[s] = h->fdecay[s];
+        }
+        CU(glz::launch_field_round(f, h->stream));
+    }
+    if (h->infect_species >= 0)
+        CU(glz::launch_infection(h->cell_type, h->dose, (int)(h->n_live ? h->cap : h->n_labels), h->infect_from,
+                                 h->infect_to, h->infect_threshold, h->n_live, h->stream));
+    if (h->has_pop)
+        if (int rc = population_launches(h, true)) return rc;
+    CU(glz::launch_engine_clock_advance(h->clock, h->g.ncol, h->stream));
+    return GLZ_OK;
+}
+
+int capture_step(glz_gpu *h) {
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = queue_clocked_step(h);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("step capture: ") + cudaGetErrorString(e));
+    const cudaError_t ei = cudaGraphInstantiate(&h->step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(GLZ_DRIVER, std::string("step graph: ") + cudaGetErrorString(ei));
+    return GLZ_OK;
+}
+
+// Steps of a direct-kernel engine, one graph replay each. The clock starts
+// from the host's counters; the host keeps them in step with every replay,
+// and checks label room before each (a growth drops the graph, whose kernels
+// hold the old arrays, and the next replay captures it anew).
+int run_graph(glz_gpu *h, uint64_t steps) {
+    glz::EngineClock c{(long long)h->mcs, (long long)h->pass_no, 0u, 0u};
+    for (int s = 0; s < h->n_species; ++s) {
+        c.field_cur |= (unsigned)(h->field_cur[s] & 1) << s;
+        c.field_flip |= (unsigned)(h->substeps[s] & 1) << s;
+    }
+    CU(cudaMemcpyAsync(h->clock, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
+    for (uint64_t r = 0; r < steps; ++r) {
+        if (h->has_pop)
+            if (int rc = ensure_capacity(h)) return rc;
+        if (!h->step_exec)
+            if (int rc = capture_step(h)) return rc;
+        CU(cudaGraphLaunch(h->step_exec, h->stream));
+        h->pass_no += (uint64_t)h->g.ncol;
+        h->mcs += 1;
+        for (int s = 0; s < h->n_species; ++s)
+            if (h->substeps[s] & 1) h->field_cur[s] = 1 - h->field_cur[s];
+        if (h->has_pop) h->n_bound = after_step(h, h->n_bound);
+    }
+    h->records_from = h->pop_steps;
+    CU(cudaStreamSynchronize(h->stream));
+    if (int rc = sync_count(h)) return rc;
     return check_error_flag(h);
 }
 
@@ -671,6 +807,7 @@ int run_band(glz_gpu *h, uint64_t steps, double *ms) {
 
 int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
     if (h->band) return run_band(h, steps, ms);
+    if (!ms && h->graph_on && h->direct && !h->resident && steps > 0) return run_graph(h, steps);
     // resident launches of at most 65536 MCS, so the barrier's arrival count
     // (blocks x passes) stays far inside 32 bits
     double total[3] = {0.0, 0.0, 0.0};
@@ -927,7 +1064,16 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     h->cell_type_host.assign(cell_type, cell_type + n_labels);
     h->n_labels = n_labels;
     find_uniform_type(h, m->contact, nt);
-    if ((rc = alloc_labels(h, h->has_pop ? kCapacityFactor * n_labels + 64 : n_labels))) return bail(rc);
+    if (h->has_pop) {
+        double least = 0.0;  // the least division volume, at least the 4 sites a division needs
+        for (int k = 0; k < nt; ++k)
+            if (divv[k] > 0.0) {
+                const double v = divv[k] < 4.0 ? 4.0 : std::ceil(divv[k]);
+                least = least == 0.0 || v < least ? v : least;
+            }
+        h->born_most = least > 0.0 ? (size_t)((double)sites / least) : 0;
+    }
+    if ((rc = alloc_labels(h, h->has_pop ? capacity_for(h, n_labels) : n_labels))) return bail(rc);
     if (h->has_pop) {
         const int n = (int)n_labels;
         if ((rc = dev_alloc(&h->n_live, 1))) return bail(rc);
@@ -967,6 +1113,8 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
         if (cudaMemset(h->pending_count, 0, sizeof(int))) return bail(fail(GLZ_DRIVER, "memset failed"));
     }
     if ((rc = dev_alloc(&h->error_flag, 1))) return bail(rc);
+    if ((rc = dev_alloc(&h->clock, 1))) return bail(rc);
+    if (const char *graph_env = std::getenv("GLAZIER_ENGINE_GRAPH")) h->graph_on = graph_env[0] != '0';
     // two counters, then a done flag per CTA for the band sweep
     if ((rc = dev_alloc(&h->barrier, 2 + 1024))) return bail(rc);
     if ((rc = dev_alloc(&h->medium, 2))) return bail(rc);
@@ -1135,11 +1283,13 @@ int glz_gpu_set_infection(glz_gpu *h, int species, int from_type, int to_type, d
     h->infect_threshold = std::llround(threshold * (double)glz::kDoseScale);
     // types now change during a run: the sweep reads them per copy
     h->uniform = -1;
+    drop_step_graph(h);  // its launches carry the rule and the uniform-type pricing
     return GLZ_OK;
 }
 
 int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len) {
     if (!h) return fail(GLZ_INVALID, "null handle");
+    drop_step_graph(h);
     if (len != 2 * (size_t)h->g.sites) {
         char msg[128];
         std::snprintf(msg, sizeof msg, "nematic field has %zu sites, the lattice %d", len / 2, h->g.sites);
@@ -1160,6 +1310,7 @@ int glz_gpu_set_nematic_field(glz_gpu *h, const double *field, size_t len) {
 
 int glz_gpu_set_nematic_field_device(glz_gpu *h, const float *field, size_t len) {
     if (!h) return fail(GLZ_INVALID, "null handle");
+    drop_step_graph(h);
     if (len != 2 * (size_t)h->g.sites) {
         char msg[128];
         std::snprintf(msg, sizeof msg, "nematic field has %zu sites, the lattice %d", len / 2, h->g.sites);
@@ -1214,6 +1365,8 @@ void glz_gpu_destroy(glz_gpu *h) {
     cudaFree(h->error_flag); cudaFree(h->medium); cudaFree(h->barrier); cudaFree(h->counters);
     free_tallies(h->t);
     free_population(h);
+    drop_step_graph(h);
+    cudaFree(h->clock);
     cudaFree(h->n_live);
     if (h->n_seen) cudaFreeHost(h->n_seen);
     for (auto &e : h->n_event)

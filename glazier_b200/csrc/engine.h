@@ -52,6 +52,17 @@ struct Tallies {
     int *anchor;         // 4 per cell (x, y, z, unused): the integer origin of the moment sums
 };
 
+// The device clock of an engine whose steps replay from one captured CUDA
+// graph: the kernels of a step read the step's number, its first pass's
+// number and each species' current field buffer here, so the same graph
+// serves every step; the graph's last node advances it.
+struct EngineClock {
+    long long step;       // Monte Carlo steps completed
+    long long pass;       // colour passes completed
+    unsigned field_cur;   // bit s: the buffer (0 or 1) holding species s
+    unsigned field_flip;  // bit s: species s takes an odd number of sub-steps, so its buffer flips each step
+};
+
 struct SweepLaunch {
     Geometry g;
     TypeTables t;
@@ -103,6 +114,13 @@ struct SweepLaunch {
     int max_ctas;            // > 0 caps the persistent grid (each CTA then walks more tiles)
     const void *tensor_map;  // CUtensorMap in device-visible memory, or null
     int *error_flag;
+    // A clocked launch (the direct kernel only) takes its step, draws, tally
+    // slots and field buffers from `clock` at run time: from this pass's
+    // colour, the seed, every tally array and the field buffers.
+    const EngineClock *clock;
+    uint64_t seed;
+    Tallies tal;
+    float *field_buf;  // two buffers per species, species-major
 };
 
 cudaError_t launch_sweep(const SweepLaunch &a, cudaStream_t stream);
@@ -201,6 +219,10 @@ struct FieldLaunch {
     int infect_species = -1;  // -1: no rule
     int infect_from;
     unsigned long long *dose;
+    // Clocked: each species' buffers from the clock's current bit and the
+    // round (`in`, `out` unused), two per species in field_buf.
+    const EngineClock *clock = nullptr;
+    float *field_buf = nullptr;
 };
 
 cudaError_t launch_field_round(const FieldLaunch &a, cudaStream_t stream);
@@ -246,6 +268,12 @@ cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream);
 // capacity.
 cudaError_t launch_settle(int2 *vs_base, long long *vs_delta, long long *mom_base, long long *mom_delta, int nm,
                           int n_labels, int tracks, const int *n_live, cudaStream_t stream);
+// The same settle at the end of a clocked step: the slots follow from the
+// clock's pass count after the step's `ncol` passes.
+cudaError_t launch_settle_clocked(const Tallies &t, int nm, int n_labels, int tracks, const int *n_live,
+                                  const EngineClock *clock, int ncol, cudaStream_t stream);
+// Advance an engine's clock by one step of `ncol` passes.
+cudaError_t launch_engine_clock_advance(EngineClock *clock, int ncol, cudaStream_t stream);
 
 // The medium's volume and unlike-bond surface, counted from the lattice
 // (the sweep keeps no tally for label 0).
@@ -265,6 +293,8 @@ struct PopulationLaunch {
     const long long *mom_base;
     const int *anchor;
     uint64_t key_death;      // stream_key(seed, step, kPopulationStream, 0)
+    const EngineClock *clock;  // clocked: the step (for the death draws) from here, with `seed`
+    uint64_t seed;
     // scratch, n_labels entries each
     unsigned char *mode;
     double *plan;            // 6 per cell: centroid, axis

@@ -71,11 +71,16 @@ __global__ void __launch_bounds__(256) field_round_kernel(const __grid_constant_
     const float faces = DIM == 3 ? 6.0f : 4.0f;
     int type = -1;
     uint32_t label = 0;
+    const unsigned cur = a.clock ? a.clock->field_cur : 0u;
     for (int s = 0; s < a.n_species; ++s) {
         if (!a.active[s]) continue;
         long long taken = 0;  // this site's uptake of the infection species, fixed point
+        // clocked: a species active in this round has flipped once a round before it
+        const unsigned from = ((cur >> s) & 1u) ^ ((unsigned)a.round & 1u);
+        float *const out = a.clock ? a.field_buf + ((size_t)2 * s + (from ^ 1u)) * (size_t)a.g.sites : a.out[s];
         if (in) {
-            const float *__restrict__ u = a.in[s];
+            const float *__restrict__ u =
+                a.clock ? a.field_buf + ((size_t)2 * s + from) * (size_t)a.g.sites : a.in[s];
             const float here = u[i];
             float sum = u[xm];
             sum = __fadd_rn(sum, u[xp]);
@@ -101,7 +106,7 @@ __global__ void __launch_bounds__(256) field_round_kernel(const __grid_constant_
                     v = v < 0.0f ? 0.0f : v;
                 }
             }
-            a.out[s][i] = v;
+            out[i] = v;
         }
         if (s == a.infect_species && a.last[s])
             add_dose(a.dose, in && type == a.infect_from ? label : kNoDose, taken);

@@ -99,7 +99,9 @@ __global__ void plan_kernel(const __grid_constant__ PopulationLaunch a) {
         p[5] = v2;
         a.mode[l] = 1;
     } else if (a.t.death_rate[t] > 0.0) {
-        if (to_f64(draw(a.key_death, (uint32_t)l)) < a.t.death_rate[t]) a.mode[l] = 2;
+        const uint64_t key =
+            a.clock ? stream_key(a.seed, (int32_t)a.clock->step, kPopulationStream, 0) : a.key_death;
+        if (to_f64(draw(key, (uint32_t)l)) < a.t.death_rate[t]) a.mode[l] = 2;
     }
 }
 

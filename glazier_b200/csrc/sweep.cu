@@ -1271,9 +1271,7 @@ __device__ __forceinline__ void pick_offset(int pick, int &dx, int &dy, int &dz)
 constexpr int kDirectCompactK = 4;
 
 template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
-__global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant__ SweepLaunch a) {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+__device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
     const int targets = (a.g.w / 2) * (a.g.h / 2) * (DIM == 3 ? a.g.d / 2 : 1);
     const PassView v{a.colour, a.key_pick, a.key_accept, a.vs_base, a.vs_prev, a.vs_cur};
     const GlobalPass acc{a, v};
@@ -1323,6 +1321,51 @@ __global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant
         }
     }
     rotate_tallies<DIM>(a);
+}
+
+template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
+__global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant__ SweepLaunch a) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    direct_sweep_body<DIM, NOFF, UNIFORM, K, EXTRAS>(a);
+}
+
+// A clocked launch's pass fields from the engine clock, as pass_launch
+// (engine.cu) sets them on the host: the step and its draws, the tally slots
+// of the pass's number, each species' current field buffer.
+__device__ __forceinline__ void clock_patch(SweepLaunch &d) {
+    const EngineClock c = *d.clock;
+    const long long p = c.pass + d.colour;
+    d.step = (int32_t)c.step;
+    d.key_pick = stream_key(d.seed, d.step, d.colour, 0);
+    d.key_accept = stream_key(d.seed, d.step, d.colour, 1);
+    d.vs_base = d.tal.vs_base[p % 2];
+    d.vs_prev = d.tal.vs_delta[(p + 2) % 3];
+    d.vs_cur = reinterpret_cast<unsigned long long *>(d.tal.vs_delta[p % 3]);
+    d.vs_next_base = d.tal.vs_base[(p + 1) % 2];
+    d.vs_clear = d.tal.vs_delta[(p + 1) % 3];
+    d.mom_base = d.tal.mom_base[p % 2];
+    d.mom_prev = d.tal.mom_delta[(p + 2) % 3];
+    d.mom_cur = reinterpret_cast<unsigned long long *>(d.tal.mom_delta[p % 3]);
+    d.mom_next_base = d.tal.mom_base[(p + 1) % 2];
+    d.mom_clear = d.tal.mom_delta[(p + 1) % 3];
+    for (int s = 0; s < d.n_species; ++s)
+        d.fields[s] = d.field_buf + ((size_t)2 * s + ((c.field_cur >> s) & 1u)) * (size_t)d.g.sites;
+}
+
+// The direct pass of a step replayed from a graph: the block copies the
+// launch into shared memory, patches it from the clock and prices from there.
+template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
+__global__ void __launch_bounds__(256) direct_sweep_clocked(const __grid_constant__ SweepLaunch a) {
+    __shared__ SweepLaunch d;
+    static_assert(sizeof(SweepLaunch) % sizeof(int) == 0, "the launch copies as words");
+    const int *src = reinterpret_cast<const int *>(&a);
+    int *dst = reinterpret_cast<int *>(&d);
+    for (int i = threadIdx.x; i < (int)(sizeof(SweepLaunch) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    if (threadIdx.x == 0) clock_patch(d);
+    __syncthreads();
+    direct_sweep_body<DIM, NOFF, UNIFORM, K, EXTRAS>(d);
 }
 
 // ---------------------------------------------------------------- the resident sweep
@@ -1685,6 +1728,15 @@ static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
     attr[0].val.programmaticStreamSerializationAllowed = programmatic_launch() && !a.has_motility;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (a.clock) {  // a step captured into a graph: plain launches, pass fields from the clock
+        cfg.numAttrs = 0;
+        if (!a.lean)
+            return compact
+                       ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
+                       : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, true>, a);
+        return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
+                       : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, false>, a);
+    }
     if (!a.lean)  // every term: length, chemotaxis, connectivity, motility, drift, nematic, moments
         return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
                        : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, true>, a);

@@ -250,10 +250,45 @@ cudaError_t launch_recount(const RecountLaunch &a, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+__device__ __forceinline__ void settle_one(int l, int2 *vs_base, long long *vs_delta, long long *mom_base,
+                                           long long *mom_delta, int nm, int tracks);
+
 __global__ void settle_kernel(int2 *vs_base, long long *vs_delta, long long *mom_base, long long *mom_delta, int nm,
                               int n, int tracks, const int *n_live) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= (n_live ? *n_live : n)) return;
+    settle_one(l, vs_base, vs_delta, mom_base, mom_delta, nm, tracks);
+}
+
+// The slots at the end of a clocked step: pass number clock->pass + ncol.
+__global__ void settle_clocked_kernel(const Tallies t, int nm, int n, int tracks, const int *n_live,
+                                      const EngineClock *clock, int ncol) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= (n_live ? *n_live : n)) return;
+    const long long p = clock->pass + ncol;
+    settle_one(l, t.vs_base[p % 2], t.vs_delta[(p + 2) % 3], t.mom_base[p % 2], t.mom_delta[(p + 2) % 3], nm, tracks);
+}
+
+__global__ void engine_clock_kernel(EngineClock *clock, int ncol) {
+    clock->step += 1;
+    clock->pass += ncol;
+    clock->field_cur ^= clock->field_flip;
+}
+
+cudaError_t launch_settle_clocked(const Tallies &t, int nm, int n_labels, int tracks, const int *n_live,
+                                  const EngineClock *clock, int ncol, cudaStream_t stream) {
+    if (n_labels <= 0) return cudaSuccess;
+    settle_clocked_kernel<<<(n_labels + 255) / 256, 256, 0, stream>>>(t, nm, n_labels, tracks, n_live, clock, ncol);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_engine_clock_advance(EngineClock *clock, int ncol, cudaStream_t stream) {
+    engine_clock_kernel<<<1, 1, 0, stream>>>(clock, ncol);
+    return cudaGetLastError();
+}
+
+__device__ __forceinline__ void settle_one(int l, int2 *vs_base, long long *vs_delta, long long *mom_base,
+                                           long long *mom_delta, int nm, int tracks) {
     int dv, ds;
     unpack_delta(vs_delta[l], dv, ds);
     int2 b = vs_base[l];
