@@ -179,6 +179,7 @@ struct glz_gpu {
     cudaGraphExec_t step_exec = nullptr;
     bool graph_on = true;
     uint64_t records_from = 0;  // count records older than this step predate graph replays
+    uint64_t arrays_version = 0;  // bumped when the per-label arrays move (a captured step then is stale)
 
     // population scratch, `cap` entries each
     unsigned char *mode = nullptr;
@@ -315,6 +316,7 @@ int alloc_labels(glz_gpu *h, size_t cap) {
     h->dose = dose;
     h->cap = cap;
     drop_step_graph(h);  // its kernels hold the old arrays
+    h->arrays_version += 1;
     return GLZ_OK;
 }
 
@@ -692,7 +694,9 @@ int queue_clocked_step(glz_gpu *h) {
     return GLZ_OK;
 }
 
-int capture_step(glz_gpu *h) {
+// One clocked step as a graph (not instantiated).
+int capture_step_graph(glz_gpu *h, cudaGraph_t *out) {
+    *out = nullptr;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     const int rc = queue_clocked_step(h);
     cudaGraph_t graph = nullptr;
@@ -702,10 +706,37 @@ int capture_step(glz_gpu *h) {
         return rc;
     }
     if (e != cudaSuccess) return fail(GLZ_DRIVER, std::string("step capture: ") + cudaGetErrorString(e));
+    *out = graph;
+    return GLZ_OK;
+}
+
+int capture_step(glz_gpu *h) {
+    cudaGraph_t graph = nullptr;
+    if (int rc = capture_step_graph(h, &graph)) return rc;
     const cudaError_t ei = cudaGraphInstantiate(&h->step_exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess) return fail(GLZ_DRIVER, std::string("step graph: ") + cudaGetErrorString(ei));
     return GLZ_OK;
+}
+
+// The clock from the host's counters, on the engine's stream.
+int upload_clock(glz_gpu *h) {
+    glz::EngineClock c{(long long)h->mcs, (long long)h->pass_no, 0u, 0u};
+    for (int s = 0; s < h->n_species; ++s) {
+        c.field_cur |= (unsigned)(h->field_cur[s] & 1) << s;
+        c.field_flip |= (unsigned)(h->substeps[s] & 1) << s;
+    }
+    CU(cudaMemcpyAsync(h->clock, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
+    return GLZ_OK;
+}
+
+// The host's counters after one replayed step.
+void advance_host(glz_gpu *h) {
+    h->pass_no += (uint64_t)h->g.ncol;
+    h->mcs += 1;
+    for (int s = 0; s < h->n_species; ++s)
+        if (h->substeps[s] & 1) h->field_cur[s] = 1 - h->field_cur[s];
+    if (h->has_pop) h->n_bound = after_step(h, h->n_bound);
 }
 
 // Steps of a direct-kernel engine, one graph replay each. The clock starts
@@ -713,25 +744,16 @@ int capture_step(glz_gpu *h) {
 // and checks label room before each (a growth drops the graph, whose kernels
 // hold the old arrays, and the next replay captures it anew).
 int run_graph(glz_gpu *h, uint64_t steps) {
-    glz::EngineClock c{(long long)h->mcs, (long long)h->pass_no, 0u, 0u};
-    for (int s = 0; s < h->n_species; ++s) {
-        c.field_cur |= (unsigned)(h->field_cur[s] & 1) << s;
-        c.field_flip |= (unsigned)(h->substeps[s] & 1) << s;
-    }
-    CU(cudaMemcpyAsync(h->clock, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
+    if (int rc = upload_clock(h)) return rc;
+    h->records_from = h->pop_steps;  // count records from before the replays say nothing of them
     for (uint64_t r = 0; r < steps; ++r) {
         if (h->has_pop)
             if (int rc = ensure_capacity(h)) return rc;
         if (!h->step_exec)
             if (int rc = capture_step(h)) return rc;
         CU(cudaGraphLaunch(h->step_exec, h->stream));
-        h->pass_no += (uint64_t)h->g.ncol;
-        h->mcs += 1;
-        for (int s = 0; s < h->n_species; ++s)
-            if (h->substeps[s] & 1) h->field_cur[s] = 1 - h->field_cur[s];
-        if (h->has_pop) h->n_bound = after_step(h, h->n_bound);
+        advance_host(h);
     }
-    h->records_from = h->pop_steps;
     CU(cudaStreamSynchronize(h->stream));
     if (int rc = sync_count(h)) return rc;
     return check_error_flag(h);
@@ -869,6 +891,43 @@ int run_steps(glz_gpu *h, uint64_t steps, double *ms) {
 }
 
 }  // namespace
+
+namespace glz {
+
+bool engine_replays(const glz_gpu *h) { return h->graph_on && h->direct && !h->resident && !h->band; }
+
+int engine_begin_replays(glz_gpu *h) {
+    if (int rc = upload_clock(h)) return rc;
+    h->records_from = h->pop_steps;
+    CU(cudaStreamSynchronize(h->stream));
+    return GLZ_OK;
+}
+
+int engine_step_graph(glz_gpu *h, cudaGraph_t *out, uint64_t *version) {
+    *version = h->arrays_version;
+    return capture_step_graph(h, out);
+}
+
+int engine_before_replay(glz_gpu *h, cudaStream_t replays, uint64_t *version) {
+    if (h->has_pop && after_step(h, h->n_bound) > h->cap) {
+        // the replays so far ran on the caller's stream: let them finish
+        // before the engine reads its count (and grows, settling on its own)
+        CU(cudaStreamSynchronize(replays));
+        if (int rc = ensure_capacity(h)) return rc;
+    }
+    *version = h->arrays_version;
+    return GLZ_OK;
+}
+
+void engine_after_replay(glz_gpu *h) { advance_host(h); }
+
+int engine_end_replays(glz_gpu *h) {
+    CU(cudaStreamSynchronize(h->stream));
+    if (int rc = sync_count(h)) return rc;
+    return check_error_flag(h);
+}
+
+}  // namespace glz
 
 extern "C" {
 

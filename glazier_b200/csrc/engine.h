@@ -306,6 +306,26 @@ struct PopulationLaunch {
 // Record the message glz_last_error() returns on this thread.
 void set_last_error(const std::string &msg);
 
+}  // namespace glz
+
+struct glz_gpu;
+
+namespace glz {
+
+// An engine's steps replayed inside another graph (the batched ensemble):
+// whether its steps replay from a captured graph at all; the clock set from
+// its counters before a run of replays; its clocked step as a graph, with the
+// version of its per-label arrays the graph holds; before each replay, room
+// for that step's divisions (syncing `replays` first when it must read its
+// count; a growth changes the version and the graph must be captured anew);
+// after each replay, its counters; after the run, its count and error flag.
+bool engine_replays(const glz_gpu *h);
+int engine_begin_replays(glz_gpu *h);
+int engine_step_graph(glz_gpu *h, cudaGraph_t *out, uint64_t *version);
+int engine_before_replay(glz_gpu *h, cudaStream_t replays, uint64_t *version);
+void engine_after_replay(glz_gpu *h);
+int engine_end_replays(glz_gpu *h);
+
 cudaError_t launch_population_plan(const PopulationLaunch &a, cudaStream_t stream);
 cudaError_t launch_population_apply(const PopulationLaunch &a, cudaStream_t stream);
 

@@ -11,6 +11,13 @@
 // chooses the persistent grid and the order replicas' tiles are dealt in by
 // time alone.
 //
+// Replicas whose models state other terms (fields, length, connectivity,
+// division, death, motility, drift, nematic) are engines of their own. When
+// their steps replay from captured graphs (the direct kernel's engines: the
+// engine clock makes one captured step serve every step), the batch's step
+// and every engine's step are child graphs of one graph, replayed once per
+// MCS; otherwise each engine steps on its own stream from a host thread.
+//
 // No reference counterpart: glazier runs one lattice per GpuSimulation.
 
 #include <cuda.h>
@@ -143,15 +150,26 @@ struct glz_ens {
     int all = 0, device = 0;
     std::vector<int> slot;
     std::vector<glz_gpu *> engines;
+    // The batch's step and every engine replica's clocked step as child
+    // graphs of one graph, replayed once per MCS; the array versions of the
+    // engines' steps it holds.
+    cudaGraphExec_t mixed = nullptr;
+    std::vector<uint64_t> versions;
 };
 
 namespace {
+
+void drop_mixed(glz_ens *h) {
+    if (h->mixed) cudaGraphExecDestroy(h->mixed);
+    h->mixed = nullptr;
+}
 
 void drop_graph(glz_ens *h) {
     if (h->exec) cudaGraphExecDestroy(h->exec);
     if (h->graph) cudaGraphDestroy(h->graph);
     h->exec = nullptr;
     h->graph = nullptr;
+    drop_mixed(h);
 }
 
 // Lay the replicas' tiles out in schedule order and upload the order.
@@ -541,10 +559,93 @@ static int which(glz_ens *h, int replica, int *batched, glz_gpu **engine) {
     return GLZ_OK;
 }
 
-// `steps` MCS of every replica: the batch on the ensemble's stream, each
-// engine on its own stream from a host thread of its own, all at once.
+// The batch's step and each engine replica's clocked step side by side in
+// one graph.
+static int build_mixed(glz_ens *h) {
+    drop_mixed(h);
+    if (h->n > 0)
+        if (int rc = build_graph(h)) return rc;
+    cudaGraph_t g = nullptr;
+    CU(cudaGraphCreate(&g, 0));
+    const auto done = [&](int rc) {
+        cudaGraphDestroy(g);
+        return rc;
+    };
+    cudaGraphNode_t node = nullptr;
+    if (h->n > 0 && cudaGraphAddChildGraphNode(&node, g, nullptr, 0, h->graph) != cudaSuccess)
+        return done(fail(GLZ_DRIVER, "cannot add the batch to the ensemble graph"));
+    h->versions.assign(h->engines.size(), 0);
+    for (size_t k = 0; k < h->engines.size(); ++k) {
+        cudaGraph_t eg = nullptr;
+        if (int rc = glz::engine_step_graph(h->engines[k], &eg, &h->versions[k])) return done(rc);
+        const cudaError_t e = cudaGraphAddChildGraphNode(&node, g, nullptr, 0, eg);
+        cudaGraphDestroy(eg);
+        if (e != cudaSuccess) return done(fail(GLZ_DRIVER, "cannot add an engine replica to the ensemble graph"));
+    }
+    if (cudaGraphInstantiate(&h->mixed, g, 0) != cudaSuccess)
+        return done(fail(GLZ_DRIVER, "cannot instantiate the ensemble graph"));
+    return done(GLZ_OK);
+}
+
+// `steps` MCS of a batch and engine replicas that all replay from graphs:
+// one replay of the mixed graph per MCS on the ensemble's stream. Before
+// each, every engine makes room for its next divisions; one whose arrays
+// grew makes the graph be captured anew.
+static int step_mixed(glz_ens *h, uint64_t steps, double *ms) {
+    for (glz_gpu *g : h->engines)
+        if (int rc = glz::engine_begin_replays(g)) return rc;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (ms) {
+        CU(cudaEventCreate(&a));
+        CU(cudaEventCreate(&b));
+        CU(cudaEventRecord(a, h->stream));
+    }
+    int rc = GLZ_OK;
+    for (uint64_t s = 0; s < steps && rc == GLZ_OK; ++s) {
+        bool stale = h->mixed == nullptr || h->versions.size() != h->engines.size();
+        for (size_t k = 0; k < h->engines.size() && rc == GLZ_OK; ++k) {
+            uint64_t v = 0;
+            rc = glz::engine_before_replay(h->engines[k], h->stream, &v);
+            stale |= rc == GLZ_OK && v != h->versions[k];
+        }
+        if (rc == GLZ_OK && stale) rc = build_mixed(h);
+        if (rc == GLZ_OK && cudaGraphLaunch(h->mixed, h->stream) != cudaSuccess)
+            rc = fail(GLZ_DRIVER, "ensemble graph launch failed");
+        if (rc != GLZ_OK) break;
+        h->step += 1;
+        h->pass += h->ncol;
+        for (glz_gpu *g : h->engines) glz::engine_after_replay(g);
+    }
+    if (ms && rc == GLZ_OK) {
+        CU(cudaEventRecord(b, h->stream));
+        CU(cudaEventSynchronize(b));
+        float t = 0.0f;
+        CU(cudaEventElapsedTime(&t, a, b));
+        *ms = t;
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(h->stream));
+    if (h->n > 0) {
+        int flag = 0;
+        CU(cudaMemcpy(&flag, h->error_flag, sizeof flag, cudaMemcpyDeviceToHost));
+        if (flag) return fail(GLZ_DRIVER, "an ensemble sweep tile reported an error (flag " + std::to_string(flag) + ")");
+    }
+    for (size_t k = 0; k < h->engines.size(); ++k)
+        if (int r = glz::engine_end_replays(h->engines[k])) return r;
+    return GLZ_OK;
+}
+
+// `steps` MCS of every replica. With engine replicas that all replay from
+// graphs, one mixed graph per MCS; otherwise the batch on the ensemble's
+// stream and each engine on its own stream from a host thread of its own,
+// all at once.
 static int step_all(glz_ens *h, uint64_t steps, double *ms) {
     if (h->engines.empty()) return run(h, steps, true, ms);
+    bool replays = true;
+    for (glz_gpu *g : h->engines) replays &= glz::engine_replays(g);
+    if (replays) return step_mixed(h, steps, ms);
     const auto t0 = std::chrono::steady_clock::now();
     const size_t e = h->engines.size();
     std::vector<int> rcs(e, GLZ_OK);
@@ -598,6 +699,7 @@ int glz_ens_set_infection(glz_ens *h, int replica, int species, int from_type, i
     glz_gpu *g = nullptr;
     if (int rc = which(h, replica, &b, &g)) return rc;
     if (!g) return fail(GLZ_UNSUPPORTED, "replica " + std::to_string(replica) + " is batched and has no fields");
+    drop_mixed(h);  // the engine's captured step carries the rule
     return glz_gpu_set_infection(g, species, from_type, to_type, threshold);
 }
 
