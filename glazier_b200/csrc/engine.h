@@ -197,7 +197,17 @@ struct EnsembleLaunch {
     int ncol;
     int uniform_contact_exact;
     int *error_flag;
+    // 0: the windowed persistent kernel (128 x 32 tiles); 1, 2, 3: one block
+    // per tile of 32 x 8, 16 x 16 or 64 x 4 targets of a plane, priced where
+    // they lie (tile_prefix and total_tiles then count those tiles)
+    int tile_shape;
 };
+
+// Targets per tile along x and y of ensemble tile shape `shape` (1, 2, 3).
+inline void ensemble_tile(int shape, int &bx, int &by) {
+    bx = shape == 1 ? 32 : (shape == 2 ? 16 : 64);
+    by = 256 / bx;
+}
 
 cudaError_t launch_ensemble_sweep(const EnsembleLaunch &e, int dim, int n_off, bool uniform, cudaStream_t stream);
 cudaError_t launch_clock_advance(EnsembleClock *clock, int ncol, cudaStream_t stream);

@@ -141,6 +141,8 @@ struct glz_ens {
     long long step = 0, pass = 0;
     int max_ctas = 0;  // 0: one full wave
     int schedule = 0;  // 0: replicas in their own order; 1: largest first
+    int tile_shape = 0;  // EnsembleLaunch::tile_shape
+    int window_tiles = 0;  // all replicas' tiles of the windowed kernel
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     // Replicas as the caller numbered them: slot[i] >= 0 is replica i's index
@@ -172,15 +174,29 @@ void drop_graph(glz_ens *h) {
     drop_mixed(h);
 }
 
-// Lay the replicas' tiles out in schedule order and upload the order.
+// A replica's tiles under a tile shape: the windowed kernel's, or the
+// direct blocks' over its targets.
+int tiles_of(const glz_ens *h, const Replica &rep, int shape) {
+    if (shape == 0) return rep.tiles;
+    int bx, by;
+    glz::ensemble_tile(shape, bx, by);
+    return ((rep.g.w / 2 + bx - 1) / bx) * ((rep.g.h / 2 + by - 1) / by);
+}
+
+// Lay the replicas' tiles out in schedule order (`schedule` bit 0: largest
+// first; bits 1-2: the tile shape) and upload the order.
 int set_schedule(glz_ens *h, int schedule, int max_ctas) {
+    const int shape = (schedule >> 1) & 3;
+    if (shape > 0 && h->dim != 2) return fail(GLZ_INVALID, "the direct tile shapes are for planes");
     std::vector<int> order(h->n);
     std::iota(order.begin(), order.end(), 0);
-    if (schedule == 1)
+    if (schedule & 1)
         std::stable_sort(order.begin(), order.end(),
                          [&](int a, int b) { return h->reps[a].tiles > h->reps[b].tiles; });
     std::vector<int> prefix(h->n + 1, 0);
-    for (int i = 0; i < h->n; ++i) prefix[i + 1] = prefix[i] + h->reps[order[i]].tiles;
+    for (int i = 0; i < h->n; ++i) prefix[i + 1] = prefix[i] + tiles_of(h, h->reps[order[i]], shape);
+    h->total_tiles = prefix[h->n];
+    h->tile_shape = shape;
     CU(cudaMemcpyAsync(h->d_order, order.data(), h->n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->d_prefix, prefix.data(), (h->n + 1) * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
@@ -194,6 +210,7 @@ glz::EnsembleLaunch launch_of(glz_ens *h, int colour) {
     glz::EnsembleLaunch e{};
     e.n = h->n;
     e.total_tiles = h->total_tiles;
+    e.tile_shape = h->tile_shape;
     e.colour = colour;
     e.max_ctas = h->max_ctas;
     e.replicas = h->d_reps;
@@ -739,9 +756,16 @@ int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice) {
     const int grids[3] = {0, cap > 2 * sms ? cap - sms : 0, sms};
     double best = 1e30;
     int best_i = 0, i = 0, rc = GLZ_OK;
+    // (schedule, grid cap): replica order x tile shape, the windowed kernel
+    // at three grid sizes, the direct shapes at one block per tile
     std::vector<std::pair<int, int>> cands;
-    for (int sch = 0; sch < 2; ++sch)
-        for (int g : grids) cands.push_back({sch, g});
+    for (int shape = 0; shape < (h->dim == 2 ? 4 : 1); ++shape)
+        for (int order = 0; order < 2; ++order) {
+            if (shape == 0)
+                for (int g : grids) cands.push_back({order, g});
+            else
+                cands.push_back({order + 2 * shape, 0});
+        }
     for (auto [sch, g] : cands) {
         if ((rc = set_schedule(h, sch, g))) break;
         double ms = 0.0;
@@ -765,7 +789,7 @@ int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice) {
 
 int glz_ens_set_schedule(glz_ens *h, int schedule, int max_ctas) {
     if (!h) return fail(GLZ_INVALID, "null handle");
-    if (schedule < 0 || schedule > 1 || max_ctas < 0) return fail(GLZ_INVALID, "no such schedule");
+    if (schedule < 0 || schedule > 7 || max_ctas < 0) return fail(GLZ_INVALID, "no such schedule");
     return h->n > 0 ? set_schedule(h, schedule, max_ctas) : GLZ_OK;
 }
 

@@ -2266,6 +2266,82 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
     }
 }
 
+// ---------------------------------------------------------------- the direct ensemble
+//
+// A plane ensemble's pass with one block per tile of BX x BY targets of one
+// replica: the block finds its replica, copies the replica's launch into
+// shared memory with the pass's fields patched from the clock, and prices
+// every target of its tile where it lies (direct_target, as the direct
+// kernel does). The tile shape sets which sites a block's loads share; the
+// autotuner picks it by time, since the results do not depend on it.
+template <int NOFF, bool UNIFORM, int BX, int BY>
+__global__ void __launch_bounds__(BX *BY) direct_ensemble_kernel(const __grid_constant__ EnsembleLaunch e) {
+    __shared__ SweepLaunch d;
+    __shared__ int where[2];  // the tile's place in the schedule, its replica
+    const long long step = e.clock->step;
+    const long long pass = e.clock->pass + e.colour;
+    const int t = blockIdx.x;
+    if (threadIdx.x == 0) {
+        const int pos = replica_of_tile(e.tile_prefix, e.n, t);
+        where[0] = pos;
+        where[1] = e.order[pos];
+    }
+    __syncthreads();
+    const int pos = where[0];
+    const EnsembleReplica &rep = e.replicas[where[1]];
+    {
+        const int *src = reinterpret_cast<const int *>(&rep.a);
+        int *dst = reinterpret_cast<int *>(&d);
+        for (int i = threadIdx.x; i < (int)(sizeof(SweepLaunch) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        d.colour = e.colour;
+        d.step = (int32_t)step;
+        d.key_pick = stream_key(rep.seed, d.step, e.colour, 0);
+        d.key_accept = stream_key(rep.seed, d.step, e.colour, 1);
+        d.vs_base = e.vs_base[pass % 2] + rep.cell_off;
+        d.vs_prev = e.vs_delta[(pass + 2) % 3] + rep.cell_off;
+        d.vs_cur = reinterpret_cast<unsigned long long *>(e.vs_delta[pass % 3] + rep.cell_off);
+    }
+    __syncthreads();
+    const int lt = t - e.tile_prefix[pos];
+    const int hw = d.g.w / 2, hh = d.g.h / 2;
+    const int tiles_x = (hw + BX - 1) / BX;
+    const int jx = (lt % tiles_x) * BX + (int)threadIdx.x % BX;
+    const int jy = (lt / tiles_x) * BY + (int)threadIdx.x / BX;
+    if (jx < hw && jy < hh) {
+        const PassView v{e.colour, d.key_pick, d.key_accept, d.vs_base, d.vs_prev, d.vs_cur};
+        direct_target<2, NOFF, UNIFORM, GlobalPass, false>(d, GlobalPass{d, v}, v.key_pick, v.key_accept,
+                                                           2 * jx + (e.colour & 1), 2 * jy + ((e.colour >> 1) & 1), 0);
+    }
+    // the tally rotation over every replica's cells, which no thread of this pass reads
+    int2 *next_base = e.vs_base[(pass + 1) % 2];
+    long long *clear = e.vs_delta[(pass + 1) % 3];
+    const int2 *base = e.vs_base[pass % 2];
+    const long long *prev = e.vs_delta[(pass + 2) % 3];
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x; l < (size_t)e.total_cells; l += stride) {
+        int dv, ds;
+        unpack_delta(prev[l], dv, ds);
+        const int2 b = base[l];
+        next_base[l] = make_int2(b.x + dv, b.y + ds);
+        clear[l] = 0;
+    }
+}
+
+template <int NOFF, bool UNIFORM>
+static cudaError_t direct_ensemble_launch(const EnsembleLaunch &e, cudaStream_t stream) {
+    if (e.total_tiles <= 0) return cudaSuccess;
+    if (e.tile_shape == 1)
+        direct_ensemble_kernel<NOFF, UNIFORM, 32, 8><<<e.total_tiles, 256, 0, stream>>>(e);
+    else if (e.tile_shape == 2)
+        direct_ensemble_kernel<NOFF, UNIFORM, 16, 16><<<e.total_tiles, 256, 0, stream>>>(e);
+    else
+        direct_ensemble_kernel<NOFF, UNIFORM, 64, 4><<<e.total_tiles, 256, 0, stream>>>(e);
+    return cudaGetLastError();
+}
+
 __global__ void clock_advance_kernel(EnsembleClock *clock, int ncol) {
     clock->step += 1;
     clock->pass += ncol;
@@ -2339,6 +2415,10 @@ static cudaError_t ensemble_launch(const EnsembleLaunch &e, cudaStream_t stream)
 
 template <bool UNIFORM>
 static cudaError_t ensemble_any(const EnsembleLaunch &e, int dim, int n_off, cudaStream_t stream) {
+    if (e.tile_shape > 0) {
+        if (dim != 2 || e.tile_shape > 3) return cudaErrorInvalidValue;
+        return n_off == 4 ? direct_ensemble_launch<4, UNIFORM>(e, stream) : direct_ensemble_launch<8, UNIFORM>(e, stream);
+    }
     if (dim == 2) {
         if (n_off == 4) return ensemble_launch<2, 4, UNIFORM>(e, stream);
         if (n_off == 8) return ensemble_launch<2, 8, UNIFORM>(e, stream);
