@@ -201,6 +201,11 @@ struct EnsembleLaunch {
     // per tile of 32 x 8, 16 x 16 or 64 x 4 targets of a plane, priced where
     // they lie (tile_prefix and total_tiles then count those tiles)
     int tile_shape;
+    // The colour schedule of the direct shapes: 0 a launch per colour pass;
+    // 1 every pass of the step in one cooperative launch, blocks striding
+    // over the tiles, a grid barrier (bounded, error flag 4) between passes.
+    int one_launch;
+    unsigned *barrier;  // [0] arrivals, [1] barriers completed; zero at launch
 };
 
 // Targets per tile along x and y of ensemble tile shape `shape` (1, 2, 3).

@@ -142,6 +142,8 @@ struct glz_ens {
     int max_ctas = 0;  // 0: one full wave
     int schedule = 0;  // 0: replicas in their own order; 1: largest first
     int tile_shape = 0;  // EnsembleLaunch::tile_shape
+    int one_launch = 0;  // EnsembleLaunch::one_launch
+    unsigned *d_barrier = nullptr;
     int window_tiles = 0;  // all replicas' tiles of the windowed kernel
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -186,8 +188,9 @@ int tiles_of(const glz_ens *h, const Replica &rep, int shape) {
 // Lay the replicas' tiles out in schedule order (`schedule` bit 0: largest
 // first; bits 1-2: the tile shape) and upload the order.
 int set_schedule(glz_ens *h, int schedule, int max_ctas) {
-    const int shape = (schedule >> 1) & 3;
+    const int shape = (schedule >> 1) & 3, one = (schedule >> 3) & 1;
     if (shape > 0 && h->dim != 2) return fail(GLZ_INVALID, "the direct tile shapes are for planes");
+    if (one && shape == 0) return fail(GLZ_INVALID, "one launch per step is a schedule of the direct tile shapes");
     std::vector<int> order(h->n);
     std::iota(order.begin(), order.end(), 0);
     if (schedule & 1)
@@ -197,6 +200,7 @@ int set_schedule(glz_ens *h, int schedule, int max_ctas) {
     for (int i = 0; i < h->n; ++i) prefix[i + 1] = prefix[i] + tiles_of(h, h->reps[order[i]], shape);
     h->total_tiles = prefix[h->n];
     h->tile_shape = shape;
+    h->one_launch = one;
     CU(cudaMemcpyAsync(h->d_order, order.data(), h->n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemcpyAsync(h->d_prefix, prefix.data(), (h->n + 1) * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     CU(cudaStreamSynchronize(h->stream));
@@ -211,6 +215,8 @@ glz::EnsembleLaunch launch_of(glz_ens *h, int colour) {
     e.n = h->n;
     e.total_tiles = h->total_tiles;
     e.tile_shape = h->tile_shape;
+    e.one_launch = h->one_launch;
+    e.barrier = h->d_barrier;
     e.colour = colour;
     e.max_ctas = h->max_ctas;
     e.replicas = h->d_reps;
@@ -228,7 +234,11 @@ glz::EnsembleLaunch launch_of(glz_ens *h, int colour) {
 
 // One Monte Carlo step of every replica: the colour launches and the clock.
 int enqueue_step(glz_ens *h) {
-    for (int c = 0; c < h->ncol; ++c) CU(glz::launch_ensemble_sweep(launch_of(h, c), h->dim, h->n_off, h->uniform, h->stream));
+    if (h->one_launch)
+        CU(glz::launch_ensemble_sweep(launch_of(h, 0), h->dim, h->n_off, h->uniform, h->stream));
+    else
+        for (int c = 0; c < h->ncol; ++c)
+            CU(glz::launch_ensemble_sweep(launch_of(h, c), h->dim, h->n_off, h->uniform, h->stream));
     CU(glz::launch_clock_advance(h->d_clock, h->ncol, h->stream));
     return GLZ_OK;
 }
@@ -384,6 +394,7 @@ static int create_batched(int n, const glz_model *models, const uint32_t *const 
         (rc = dev_alloc(&h->anchor, cells * 4)) || (rc = dev_alloc(&h->d_reps, (size_t)n)) ||
         (rc = dev_alloc(&h->d_maps, (size_t)n)) || (rc = dev_alloc(&h->d_prefix, (size_t)n + 1)) ||
         (rc = dev_alloc(&h->d_order, (size_t)n)) || (rc = dev_alloc(&h->d_clock, 1)) ||
+        (rc = dev_alloc(&h->d_barrier, 2)) ||
         (rc = dev_alloc(&h->error_flag, 1)) || (rc = dev_alloc(&h->medium, 2)))
         return bail(rc);
     // per-type tables, one block per replica: contact (n_types^2), tv, lv, ts, ls
@@ -761,10 +772,12 @@ int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice) {
     std::vector<std::pair<int, int>> cands;
     for (int shape = 0; shape < (h->dim == 2 ? 4 : 1); ++shape)
         for (int order = 0; order < 2; ++order) {
-            if (shape == 0)
+            if (shape == 0) {
                 for (int g : grids) cands.push_back({order, g});
-            else
-                cands.push_back({order + 2 * shape, 0});
+            } else {
+                cands.push_back({order + 2 * shape, 0});      // a launch per colour pass
+                cands.push_back({order + 2 * shape + 8, 0});  // the step's passes in one launch
+            }
         }
     for (auto [sch, g] : cands) {
         if ((rc = set_schedule(h, sch, g))) break;
@@ -789,7 +802,7 @@ int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice) {
 
 int glz_ens_set_schedule(glz_ens *h, int schedule, int max_ctas) {
     if (!h) return fail(GLZ_INVALID, "null handle");
-    if (schedule < 0 || schedule > 7 || max_ctas < 0) return fail(GLZ_INVALID, "no such schedule");
+    if (schedule < 0 || schedule > 15 || max_ctas < 0) return fail(GLZ_INVALID, "no such schedule");
     return h->n > 0 ? set_schedule(h, schedule, max_ctas) : GLZ_OK;
 }
 
@@ -870,7 +883,7 @@ void glz_ens_destroy(glz_ens *h) {
     for (auto *p : h->vs_delta) cudaFree(p);
     cudaFree(h->volc); cudaFree(h->anchor); cudaFree(h->tables); cudaFree(h->connected);
     cudaFree(h->d_reps); cudaFree(h->d_maps); cudaFree(h->d_prefix); cudaFree(h->d_order);
-    cudaFree(h->d_clock); cudaFree(h->error_flag); cudaFree(h->medium);
+    cudaFree(h->d_clock); cudaFree(h->d_barrier); cudaFree(h->error_flag); cudaFree(h->medium);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

@@ -2274,13 +2274,12 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
 // every target of its tile where it lies (direct_target, as the direct
 // kernel does). The tile shape sets which sites a block's loads share; the
 // autotuner picks it by time, since the results do not depend on it.
+// Tile t of colour pass `colour` (pass number `pass`, step `step`): the
+// block finds the tile's replica, patches the replica's launch into `d` and
+// prices the tile's targets.
 template <int NOFF, bool UNIFORM, int BX, int BY>
-__global__ void __launch_bounds__(BX *BY) direct_ensemble_kernel(const __grid_constant__ EnsembleLaunch e) {
-    __shared__ SweepLaunch d;
-    __shared__ int where[2];  // the tile's place in the schedule, its replica
-    const long long step = e.clock->step;
-    const long long pass = e.clock->pass + e.colour;
-    const int t = blockIdx.x;
+__device__ __forceinline__ void direct_ensemble_tile(const EnsembleLaunch &e, SweepLaunch &d, int *where, int t,
+                                                     int colour, long long step, long long pass) {
     if (threadIdx.x == 0) {
         const int pos = replica_of_tile(e.tile_prefix, e.n, t);
         where[0] = pos;
@@ -2296,10 +2295,10 @@ __global__ void __launch_bounds__(BX *BY) direct_ensemble_kernel(const __grid_co
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        d.colour = e.colour;
+        d.colour = colour;
         d.step = (int32_t)step;
-        d.key_pick = stream_key(rep.seed, d.step, e.colour, 0);
-        d.key_accept = stream_key(rep.seed, d.step, e.colour, 1);
+        d.key_pick = stream_key(rep.seed, d.step, colour, 0);
+        d.key_accept = stream_key(rep.seed, d.step, colour, 1);
         d.vs_base = e.vs_base[pass % 2] + rep.cell_off;
         d.vs_prev = e.vs_delta[(pass + 2) % 3] + rep.cell_off;
         d.vs_cur = reinterpret_cast<unsigned long long *>(e.vs_delta[pass % 3] + rep.cell_off);
@@ -2311,11 +2310,16 @@ __global__ void __launch_bounds__(BX *BY) direct_ensemble_kernel(const __grid_co
     const int jx = (lt % tiles_x) * BX + (int)threadIdx.x % BX;
     const int jy = (lt / tiles_x) * BY + (int)threadIdx.x / BX;
     if (jx < hw && jy < hh) {
-        const PassView v{e.colour, d.key_pick, d.key_accept, d.vs_base, d.vs_prev, d.vs_cur};
+        const PassView v{colour, d.key_pick, d.key_accept, d.vs_base, d.vs_prev, d.vs_cur};
         direct_target<2, NOFF, UNIFORM, GlobalPass, false>(d, GlobalPass{d, v}, v.key_pick, v.key_accept,
-                                                           2 * jx + (e.colour & 1), 2 * jy + ((e.colour >> 1) & 1), 0);
+                                                           2 * jx + (colour & 1), 2 * jy + ((colour >> 1) & 1), 0);
     }
-    // the tally rotation over every replica's cells, which no thread of this pass reads
+    __syncthreads();  // `d` and `where` serve the block's next tile
+}
+
+// The tally rotation over every replica's cells for the pass numbered `pass`,
+// which no thread of that pass reads, spread over the grid.
+__device__ __forceinline__ void ensemble_rotate(const EnsembleLaunch &e, long long pass) {
     int2 *next_base = e.vs_base[(pass + 1) % 2];
     long long *clear = e.vs_delta[(pass + 1) % 3];
     const int2 *base = e.vs_base[pass % 2];
@@ -2330,16 +2334,70 @@ __global__ void __launch_bounds__(BX *BY) direct_ensemble_kernel(const __grid_co
     }
 }
 
+// A plane ensemble's pass with one block per tile of BX x BY targets of one
+// replica, priced where they lie (direct_target, as the direct kernel does).
+// The tile shape sets which sites a block's loads share; the autotuner picks
+// it by time, since the results do not depend on it.
+template <int NOFF, bool UNIFORM, int BX, int BY>
+__global__ void __launch_bounds__(BX *BY) direct_ensemble_kernel(const __grid_constant__ EnsembleLaunch e) {
+    __shared__ SweepLaunch d;
+    __shared__ int where[2];  // the tile's place in the schedule, its replica
+    const long long step = e.clock->step;
+    const long long pass = e.clock->pass + e.colour;
+    direct_ensemble_tile<NOFF, UNIFORM, BX, BY>(e, d, where, (int)blockIdx.x, e.colour, step, pass);
+    ensemble_rotate(e, pass);
+}
+
+// Every colour pass of a step in one cooperative launch: blocks stride over
+// the tiles, a grid barrier between passes (the tallies a pass reads are its
+// snapshot, complete once every block has finished the pass before).
+template <int NOFF, bool UNIFORM, int BX, int BY>
+__global__ void __launch_bounds__(BX *BY) direct_ensemble_step_kernel(const __grid_constant__ EnsembleLaunch e) {
+    __shared__ SweepLaunch d;
+    __shared__ int where[2];
+    const long long step = e.clock->step;
+    for (int c = 0; c < e.ncol; ++c) {
+        const long long pass = e.clock->pass + c;
+        for (int t = (int)blockIdx.x; t < e.total_tiles; t += (int)gridDim.x)
+            direct_ensemble_tile<NOFF, UNIFORM, BX, BY>(e, d, where, t, c, step, pass);
+        ensemble_rotate(e, pass);
+        if (c + 1 < e.ncol && !resident_barrier(e.barrier, (unsigned)c)) {
+            if (threadIdx.x == 0) atomicExch(e.error_flag, 4);
+            return;
+        }
+    }
+}
+
+template <int NOFF, bool UNIFORM, int BX, int BY>
+static cudaError_t direct_ensemble_shape(const EnsembleLaunch &e, cudaStream_t stream) {
+    if (!e.one_launch) {
+        direct_ensemble_kernel<NOFF, UNIFORM, BX, BY><<<e.total_tiles, BX * BY, 0, stream>>>(e);
+        return cudaGetLastError();
+    }
+    static int most = 0;  // blocks that can all be resident at once
+    if (!most) {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaError_t x = cudaGetDevice(&dev)) return x;
+        if (cudaError_t x = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return x;
+        if (cudaError_t x = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, direct_ensemble_step_kernel<NOFF, UNIFORM, BX, BY>, BX * BY, 0))
+            return x;
+        most = sms * per_sm;
+    }
+    if (most < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int grid = e.total_tiles < most ? e.total_tiles : most;
+    if (cudaError_t x = cudaMemsetAsync(e.barrier, 0, 2 * sizeof(unsigned), stream)) return x;
+    void *args[] = {const_cast<EnsembleLaunch *>(&e)};
+    return cudaLaunchCooperativeKernel((const void *)direct_ensemble_step_kernel<NOFF, UNIFORM, BX, BY>, dim3(grid),
+                                       dim3(BX * BY), args, 0, stream);
+}
+
 template <int NOFF, bool UNIFORM>
 static cudaError_t direct_ensemble_launch(const EnsembleLaunch &e, cudaStream_t stream) {
     if (e.total_tiles <= 0) return cudaSuccess;
-    if (e.tile_shape == 1)
-        direct_ensemble_kernel<NOFF, UNIFORM, 32, 8><<<e.total_tiles, 256, 0, stream>>>(e);
-    else if (e.tile_shape == 2)
-        direct_ensemble_kernel<NOFF, UNIFORM, 16, 16><<<e.total_tiles, 256, 0, stream>>>(e);
-    else
-        direct_ensemble_kernel<NOFF, UNIFORM, 64, 4><<<e.total_tiles, 256, 0, stream>>>(e);
-    return cudaGetLastError();
+    if (e.tile_shape == 1) return direct_ensemble_shape<NOFF, UNIFORM, 32, 8>(e, stream);
+    if (e.tile_shape == 2) return direct_ensemble_shape<NOFF, UNIFORM, 16, 16>(e, stream);
+    return direct_ensemble_shape<NOFF, UNIFORM, 64, 4>(e, stream);
 }
 
 __global__ void clock_advance_kernel(EnsembleClock *clock, int ncol) {

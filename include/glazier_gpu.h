@@ -220,13 +220,16 @@ int glz_ens_set_infection(glz_ens *h, int replica, int species, int from_type, i
 /* Time each schedule on a snapshot of the state for `trial_steps` steps,
  * restore the state, keep the fastest: replica order x tile shape (the
  * windowed persistent kernel's 128 x 32 tiles at three grid sizes, and for
- * planes blocks of 32 x 8, 16 x 16 or 64 x 4 targets priced where they
- * lie). `choice` gets the index of the candidate kept. */
+ * planes blocks of 32 x 8, 16 x 16 or 64 x 4 targets priced where they lie)
+ * x colour schedule for those blocks (a launch per colour pass, or a step's
+ * passes in one cooperative launch with a grid barrier between them).
+ * `choice` gets the index of the candidate kept. */
 int glz_ens_autotune(glz_ens *h, uint64_t trial_steps, int *choice);
 /* Choose a schedule directly: bit 0 the replica order (0 as given, 1 largest
  * first), bits 1-2 the tile shape (0 windowed, 1 32 x 8, 2 16 x 16, 3 64 x 4;
- * 1-3 for planes only); max_ctas caps the windowed kernel's grid (0 for one
- * full wave). Results do not depend on it. */
+ * 1-3 for planes only), bit 3 the step's passes in one launch (shapes 1-3
+ * only); max_ctas caps the windowed kernel's grid (0 for one full wave).
+ * Results do not depend on it. */
 int glz_ens_set_schedule(glz_ens *h, int schedule, int max_ctas);
 int glz_ens_labels(glz_ens *h, int replica, uint32_t *out, size_t sites);
 int glz_ens_volumes(glz_ens *h, int replica, uint32_t *out, size_t *count);

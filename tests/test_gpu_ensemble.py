@@ -67,8 +67,10 @@ def test_a_replica_matches_the_host_replay(device):
 
 
 # schedule bit 0: replica order; bits 1-2: tile shape (0 windowed, 1-3 direct
-# blocks of 32 x 8, 16 x 16, 64 x 4 targets)
-@pytest.mark.parametrize("schedule,ctas", [(0, 0), (1, 0), (0, 3), (1, 7), (2, 0), (3, 0), (4, 0), (7, 0)])
+# blocks of 32 x 8, 16 x 16, 64 x 4 targets); bit 3: a step's passes in one
+# cooperative launch
+@pytest.mark.parametrize("schedule,ctas", [(0, 0), (1, 0), (0, 3), (1, 7), (2, 0), (3, 0), (4, 0), (7, 0), (10, 0),
+                                           (13, 0), (15, 0)])
 def test_the_schedule_changes_only_the_time(device, schedule, ctas):
     from glazier_b200.ensemble import Ensemble
 
