@@ -71,7 +71,7 @@ struct BandLaunch {
 
 struct BandHead {
     alignas(8) unsigned long long full[kBandMaxSlots];   // the slot's row has landed
-    alignas(8) unsigned long long empty[kBandMaxSlots];  // every consumer is done with the slot's row
+    alignas(8) unsigned long long empty[kBandMaxSlots];  // every consumer warp is done with the slot's row
     unsigned last[kBandMaxSlots];  // sequence number of the latest row put into the slot, plus one
     float contact[kBandTypes * kBandTypes];
     int abort;   // a wait gave up: every warp stops at the pass's end
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
     if (tid == 0) {
         for (int s = 0; s < slots; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.full[s])));
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&S.empty[s])), "r"(kBandConsumers));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&S.empty[s])), "r"(kBandWarps));
             S.last[s] = 0;
         }
         S.abort = 0;
@@ -413,9 +413,15 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                 const auto ready = [&](uint32_t q) {
                     return band_wait(&S.full[q % (uint32_t)slots], (q / (uint32_t)slots) & 1u);
                 };
+                // One arrival per warp: the warp's lanes meet first (their reads of
+                // the slot come before lane 0's arrival), so a slot takes as many
+                // arrivals as there are consumer warps, not threads.
                 const auto release = [&](uint32_t q) {
-                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&S.empty[q % (uint32_t)slots]))
-                                 : "memory");
+                    __syncwarp();
+                    if (lane == 0)
+                        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                         smem_addr(&S.empty[q % (uint32_t)slots]))
+                                     : "memory");
                 };
                 // entries held over from the previous target row: queue[0, held), its rows and y
                 int held = 0, hy = 0;
@@ -437,8 +443,8 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
                     // Light pass: the warp's targets whose pick carries another label
                     // join its queue behind the entries held from the previous row.
                     int total = held;
-                    for (int k = 0; k < per_row; ++k) {
-                        const int i = (k * kBandWarps + warp) * 32 + lane;
+                    for (int part = 0; part < per_row; ++part) {
+                        const int i = (part * kBandWarps + warp) * 32 + lane;
                         bool active = false;
                         int pick = 0;
                         if (i < HW) {

@@ -634,7 +634,7 @@ static int step_mixed(glz_ens *h, uint64_t steps, double *ms) {
         for (size_t k = 0; k < h->engines.size() && rc == GLZ_OK; ++k) {
             uint64_t v = 0;
             rc = glz::engine_before_replay(h->engines[k], h->stream, &v);
-            stale |= rc == GLZ_OK && v != h->versions[k];
+            stale |= rc == GLZ_OK && (k >= h->versions.size() || v != h->versions[k]);
         }
         if (rc == GLZ_OK && stale) rc = build_mixed(h);
         if (rc == GLZ_OK && cudaGraphLaunch(h->mixed, h->stream) != cudaSuccess)
