@@ -183,8 +183,9 @@ def mixed_ensemble_compare(mcs: int, device: int) -> dict:
     """The configuration's full mix: 64 replicas alternating the plain
     monolayer and the two-field infection model (sides log-uniform 128..1024,
     own T, J and lambda_V; `mixed_ensemble_starts`). The monolayers run as
-    one batch, each infection model as its own engine beside it; against
-    looping the plain engine over the same replicas. Wall clock to every
+    one batch and each infection model as an engine whose captured step sits
+    beside the batch's in one graph, replayed once per MCS; against looping
+    the plain engine over the same replicas. Wall clock to every
     replica's result, both ways; a batched and an infection replica compared
     for identity."""
     import torch
@@ -220,8 +221,8 @@ def mixed_ensemble_compare(mcs: int, device: int) -> dict:
     ens.close()
     return {"replicas": 64, "infection_replicas": len(infected), "sites": sites, "mcs": mcs, "mixed_s": mixed_s,
             "looped_plain_s": looped_s, "speedup": looped_s / mixed_s, "lattices_identical": bool(same),
-            "note": "monolayers batched in one persistent launch per colour; infection models as engines on their "
-                    "own streams beside it"}
+            "note": "monolayers batched (autotuned tile shape and colour schedule); each infection model's clocked "
+                    "step beside the batch's, one graph replay per MCS for all 64"}
 
 
 def adjoint_compare(steps: int, every: int, repeats: int, device: int) -> dict:
