@@ -59,7 +59,11 @@ constexpr bool kBandOverlap = GLZ_BAND_OVERLAP != 0;
 // The barrier words: [0] arrivals, [1] barriers completed, then per CTA the
 // passes it has completed in this launch.
 constexpr int kBandMaxGrid = 1024;
+#ifndef GLZ_BAND_PER_SM
+#define GLZ_BAND_PER_SM 1
+#endif
 constexpr int kBandWarps = GLZ_BAND_WARPS;  // consumer warps; one more warp produces
+constexpr int kBandPerSm = GLZ_BAND_PER_SM;  // CTAs (bands) per SM, each with its share of shared memory
 constexpr int kBandThreads = 32 * (kBandWarps + 1);
 constexpr int kBandConsumers = 32 * kBandWarps;
 
@@ -251,7 +255,7 @@ __device__ __forceinline__ bool band_barrier(unsigned *bar, unsigned k, int *ok_
 }
 
 template <int NOFF, bool UNIFORM>
-__global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __grid_constant__ BandLaunch B) {
+__global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(const __grid_constant__ BandLaunch B) {
     const ResidentLaunch &r = B.r;
     const SweepLaunch &a = r.a;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -550,6 +554,16 @@ __global__ void __launch_bounds__(kBandThreads, 1) band_sweep_kernel(const __gri
     }
 }
 
+// The shared memory a band's CTA may take: the per-block limit, or its share
+// of the SM's when several CTAs share one.
+static int band_budget(int dev) {
+    int optin = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) return 0;
+    const int share = per_sm / kBandPerSm - 1024;  // each resident block also holds 1 KB the system reserves
+    return share < optin ? share : optin;
+}
+
 // The launch shape of the band sweep for a plane of width w: ring rows and
 // queue room, or false when the plane does not suit it.
 static bool band_shape(int w, int h, int smem_optin, int &slots, int &qcap, size_t &smem) {
@@ -574,7 +588,7 @@ static cudaError_t launch_band(const ResidentLaunch &r, cudaStream_t stream) {
         int dev = 0;
         if (cudaError_t e = cudaGetDevice(&dev)) return e;
         if (cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return e;
-        if (cudaError_t e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) return e;
+        optin = band_budget(dev);
     }
     BandLaunch b{};
     b.r = r;
@@ -587,16 +601,16 @@ static cudaError_t launch_band(const ResidentLaunch &r, cudaStream_t stream) {
     if (cudaError_t e =
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_sweep_kernel<NOFF, UNIFORM>, kBandThreads, smem))
         return e;
-    if (per_sm < 1 || sms > kBandMaxGrid) return cudaErrorNotSupported;
+    if (per_sm < kBandPerSm || sms * kBandPerSm > kBandMaxGrid) return cudaErrorNotSupported;
     void *args[] = {&b};
-    return cudaLaunchCooperativeKernel((const void *)band_sweep_kernel<NOFF, UNIFORM>, dim3((unsigned)sms),
-                                       dim3(kBandThreads), args, smem, stream);
+    return cudaLaunchCooperativeKernel((const void *)band_sweep_kernel<NOFF, UNIFORM>,
+                                       dim3((unsigned)(sms * kBandPerSm)), dim3(kBandThreads), args, smem, stream);
 }
 
 bool band_sweep_fits(int w, int h) {
-    int dev = 0, optin = 0;
+    int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
-    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+    const int optin = band_budget(dev);
     int slots = 0, qcap = 0;
     size_t smem = 0;
     return band_shape(w, h, optin, slots, qcap, smem);
