@@ -257,8 +257,9 @@ def test_the_adjoint_matches_at_the_benchmark_shape(device):
     engine, two fields from zero, checkpoints every 10 steps, the MSE against
     the f64 forward at parameters perturbed by 10% uniform noise. The f32
     adjoint gradient is within 1e-4 (infinity norm, relative) of f64 autograd
-    of the plain stencil and of FP64 central differences (h = 1e-6), both run
-    on the GPU in f64."""
+    of the plain stencil, and within 1e-4 of FP64 central differences
+    (h = 1e-6) beyond their own distance from autograd, all run on the GPU in
+    f64."""
     import torch
 
     from glazier_b200.adjoint import FieldAdjoint, owner_types
@@ -309,6 +310,10 @@ def test_the_adjoint_matches_at_the_benchmark_shape(device):
             up[i] += h
             dn[i] -= h
             fd[i] = (loss(torch.from_numpy(up).to(dev)).item() - loss(torch.from_numpy(dn).to(dev)).item()) / (2 * h)
+    # At this shape the differences carry an error of their own: exact f64
+    # autograd is about 2.2e-4 (relative, infinity norm) from them, and the
+    # adjoint, within 1e-4 of autograd, sits as close to them as autograd
+    # does. The bar is the differences' own distance from autograd plus 1e-4.
     rel_fd = float(np.abs(gp - fd).max() / np.abs(fd).max())
     auto_fd = float(np.abs(auto - fd).max() / np.abs(fd).max())
-    assert rel_fd < 1e-4, f"adjoint vs central differences {rel_fd:.3e} (autograd vs them {auto_fd:.3e})"
+    assert rel_fd < auto_fd + 1e-4, f"adjoint vs central differences {rel_fd:.3e} (autograd vs them {auto_fd:.3e})"
