@@ -279,6 +279,20 @@ def adjoint_compare(steps: int, every: int, repeats: int, device: int) -> dict:
             "note": "fields are 1 MB each: the working set sits in L2, so HBM is not the bound here"}
 
 
+def _device_ms(sim, run, device: int) -> float:
+    """Milliseconds of device time `run` takes on the engine's stream."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(sim.stream, device=f"cuda:{device}")
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    run()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
 def infection_compare(mcs: int, cpu_mcs: int, device: int) -> dict:
     """The two-field infection model at 256^2 (centred 16 x 16 tissue with one
     infected cell, 32 immune cells at random in the medium; fields, division,
@@ -293,20 +307,27 @@ def infection_compare(mcs: int, cpu_mcs: int, device: int) -> dict:
 
     start = infection_start()
     sites = start.model.sites
+    # the default path: every step replayed from the engine's captured graph,
+    # device time by events on its stream around the whole run
     sim = GpuSimulation.from_start(start, device=device)
     sim.set_infection(*INFECTION_RULE)
-    ms = sim.step_profiled(mcs)
+    total = _device_ms(sim, lambda: sim.step(mcs), device)
     types, vols = sim.cell_types(), sim.volumes()
     infected = int(((types == 2) & (vols > 0)).sum())
     cells = int((vols[1:] > 0).sum())
     sim.close()
-    total = sum(ms)
+    # the phases, from a second run of the same start with every launch queued
+    # from the host and each phase bracketed by events
+    sim = GpuSimulation.from_start(start, device=device)
+    sim.set_infection(*INFECTION_RULE)
+    ms = sim.step_profiled(mcs)
+    sim.close()
     o = SerialOracle.from_start(start)
     t = time.perf_counter()
     o.step(cpu_mcs)
     cpu_s = time.perf_counter() - t
     return {"lattice": "256x256", "mcs": mcs, "device_ms": total,
-            "phase_ms": {"sweep": ms[0], "fields": ms[1], "population": ms[2]},
+            "phase_ms": {"sweep": ms[0], "fields": ms[1], "population": ms[2], "run": "host-queued launches"},
             "site_updates_per_s": sites * mcs / (total / 1e3), "live_cells_end": cells,
             "infected_end": infected,
             "cpu_serial": {"mcs": cpu_mcs, "seconds": cpu_s, "site_updates_per_s": sites * cpu_mcs / cpu_s,
@@ -346,20 +367,20 @@ def published_rows(device: int) -> dict:
         sim = GpuSimulation.from_start(Start.tiled(m, 8), device=device)
         torch.cuda.synchronize()
         t = time.perf_counter()
-        ms = sim.step_profiled(100)
+        dev_ms = _device_ms(sim, lambda: sim.step(100), device)
         wall = time.perf_counter() - t
         sim.close()
-        rows[f"{size}^2"] = {"mcs": 100, "wall_s": wall, "device_ms": sum(ms), "published_s": published,
+        rows[f"{size}^2"] = {"mcs": 100, "wall_s": wall, "device_ms": dev_ms, "published_s": published,
                              "site_updates_per_s": size * size * 100 / wall, "speedup": published / wall}
     texts = json.loads((ROOT / "tests" / "golden" / "serial_reference.json").read_text())["parse"]
     for name, (steps, published) in PUBLISHED_BLUEPRINTS.items():
         session = native.GpuSession(texts[name]["text"])
         torch.cuda.synchronize()
         t = time.perf_counter()
-        ms = session.simulation.step_profiled(steps)
+        dev_ms = _device_ms(session.simulation, lambda: session.simulation.step(steps), device)
         wall = time.perf_counter() - t
         session.simulation.close()
-        rows[name] = {"mcs": steps, "wall_s": wall, "device_ms": sum(ms), "published_s": published,
+        rows[name] = {"mcs": steps, "wall_s": wall, "device_ms": dev_ms, "published_s": published,
                       "speedup": published / wall}
     return rows
 
