@@ -41,7 +41,7 @@ namespace glz {
 
 constexpr int kBandPad = 4;         // labels of periodic halo at each end of a ring row (16 bytes)
 constexpr int kBandMaxSlots = 16;   // ring rows at most
-constexpr int kBandMinSlots = 6;    // three rows in use and three in flight at least
+constexpr int kBandMinSlots = 8;    // five rows in use (a target row's three, the last one's two) and three ahead
 constexpr int kBandTypes = 16;      // contact tables up to 16 types live in shared memory
 constexpr long long kBandWaitLimit = 1LL << 20;     // mbarrier polls before a wait gives up
 constexpr long long kBandBarrierLimit = 1LL << 22;  // grid-barrier polls (each an L2 round trip)
@@ -69,7 +69,8 @@ constexpr int kBandConsumers = 32 * kBandWarps;
 
 struct BandLaunch {
     ResidentLaunch r;
-    int slots;  // ring rows
+    int slots;  // ring rows, a power of two
+    int shift;  // log2(slots)
     int qcap;   // queue entries per consumer warp
 };
 
@@ -102,9 +103,13 @@ __device__ __forceinline__ unsigned band_load_acquire(const unsigned *p) {
 }
 
 // Wait (bounded) until the word at p reaches `want`: false if it gave up.
+// Each poll after the first few sleeps a little, so a waiting warp does not
+// take issue slots from the warps still at work.
 __device__ __forceinline__ bool band_wait_word(const unsigned *p, unsigned want) {
-    for (long long spin = 0; spin < kBandBarrierLimit; ++spin)
+    for (long long spin = 0; spin < kBandBarrierLimit; ++spin) {
         if (band_load_acquire(p) >= want) return true;
+        if (spin >= 4) __nanosleep(64);
+    }
     return false;
 }
 
@@ -263,6 +268,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
     unsigned char *base = smem_raw + ((128u - (raw & 127u)) & 127u);
     BandHead &S = *reinterpret_cast<BandHead *>(base);
     const int slots = B.slots, qcap = B.qcap;
+    const uint32_t mask = (uint32_t)slots - 1u, shift = (uint32_t)B.shift;  // slot q & mask, its use q >> shift
     uint32_t *queues = reinterpret_cast<uint32_t *>(base + ((sizeof(BandHead) + 127) / 128) * 128);
     const int W = a.g.w, H = a.g.h;
     const int RW = W + 2 * kBandPad;
@@ -311,8 +317,8 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
                     for (int j = 0; j < rows; ++j) {
                         if (*(volatile int *)&S.abort) break;
                         const uint32_t q = q0 + (uint32_t)j;
-                        const int slot = (int)(q % (uint32_t)slots);
-                        const uint32_t use = q / (uint32_t)slots;
+                        const int slot = (int)(q & mask);
+                        const uint32_t use = q >> shift;
                         if (use > 0 && !band_wait(&S.empty[slot], (use - 1u) & 1u)) {
                             atomicExch(a.error_flag, 1);
                             S.abort = 1;
@@ -390,6 +396,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
                                         break;
                                     }
                                     if (*(volatile int *)&S.abort) break;
+                                    __nanosleep(64);
                                 }
                             }
                             if (!ok) {
@@ -413,10 +420,8 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
                     return true;
                 };
                 if (!kBandOverlap) sync_pass();
-                const auto row_of = [&](uint32_t q) { return ring + (size_t)(q % (uint32_t)slots) * RW + kBandPad; };
-                const auto ready = [&](uint32_t q) {
-                    return band_wait(&S.full[q % (uint32_t)slots], (q / (uint32_t)slots) & 1u);
-                };
+                const auto row_of = [&](uint32_t q) { return ring + (size_t)(q & mask) * RW + kBandPad; };
+                const auto ready = [&](uint32_t q) { return band_wait(&S.full[q & mask], (q >> shift) & 1u); };
                 // One arrival per warp: the warp's lanes meet first (their reads of
                 // the slot come before lane 0's arrival), so a slot takes as many
                 // arrivals as there are consumer warps, not threads.
@@ -424,7 +429,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
                     __syncwarp();
                     if (lane == 0)
                         asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
-                                         smem_addr(&S.empty[q % (uint32_t)slots]))
+                                         smem_addr(&S.empty[q & mask]))
                                      : "memory");
                 };
                 // entries held over from the previous target row: queue[0, held), its rows and y
@@ -530,7 +535,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
                 // let every copy still in flight land before the block leaves
                 if (producer && lane == 0)
                     for (int s = 0; s < slots; ++s)
-                        if (S.last[s] > 0) band_wait(&S.full[s], ((S.last[s] - 1u) / (uint32_t)slots) & 1u);
+                        if (S.last[s] > 0) band_wait(&S.full[s], ((S.last[s] - 1u) >> shift) & 1u);
                 __syncthreads();
                 return;
             }
@@ -566,7 +571,7 @@ static int band_budget(int dev) {
 
 // The launch shape of the band sweep for a plane of width w: ring rows and
 // queue room, or false when the plane does not suit it.
-static bool band_shape(int w, int h, int smem_optin, int &slots, int &qcap, size_t &smem) {
+static bool band_shape(int w, int h, int smem_optin, int &slots, int &shift, int &qcap, size_t &smem) {
     if (w % 4 != 0 || w < 2 * kBandPad || h < 2 || w / 2 > 0xffff) return false;
     const int per_row = (w / 2 + 32 * kBandWarps - 1) / (32 * kBandWarps);
     qcap = 32 * per_row + 32;
@@ -575,8 +580,16 @@ static bool band_shape(int w, int h, int smem_optin, int &slots, int &qcap, size
     const size_t row = (size_t)(w + 2 * kBandPad) * 4;
     const long long room = (long long)smem_optin - 128 - (long long)head - (long long)queue;
     if (room < (long long)row * kBandMinSlots) return false;
-    slots = (int)(room / (long long)row);
-    if (slots > kBandMaxSlots) slots = kBandMaxSlots;
+    // the most rows that fit, rounded down to a power of two so a row's slot
+    // and phase are a mask and a shift of its sequence number
+    const long long fit = room / (long long)row;
+    slots = 1;
+    shift = 0;
+    while (2LL * slots <= fit && 2 * slots <= kBandMaxSlots) {
+        slots *= 2;
+        ++shift;
+    }
+    if (slots < kBandMinSlots) return false;
     smem = head + queue + (size_t)slots * row + 128;
     return true;
 }
@@ -593,7 +606,7 @@ static cudaError_t launch_band(const ResidentLaunch &r, cudaStream_t stream) {
     BandLaunch b{};
     b.r = r;
     size_t smem = 0;
-    if (!band_shape(r.a.g.w, r.a.g.h, optin, b.slots, b.qcap, smem)) return cudaErrorNotSupported;
+    if (!band_shape(r.a.g.w, r.a.g.h, optin, b.slots, b.shift, b.qcap, smem)) return cudaErrorNotSupported;
     if (cudaError_t e = cudaFuncSetAttribute(band_sweep_kernel<NOFF, UNIFORM>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))
         return e;
@@ -611,9 +624,9 @@ bool band_sweep_fits(int w, int h) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     const int optin = band_budget(dev);
-    int slots = 0, qcap = 0;
+    int slots = 0, shift = 0, qcap = 0;
     size_t smem = 0;
-    return band_shape(w, h, optin, slots, qcap, smem);
+    return band_shape(w, h, optin, slots, shift, qcap, smem);
 }
 
 cudaError_t launch_band_sweep(const ResidentLaunch &r, cudaStream_t stream) {
