@@ -7,28 +7,27 @@
 // so a run is bit for bit the one they and the host replay give.
 //
 // Layout of the work:
-//   - One CTA per SM owns a fixed band of each pass's target rows (the rows
-//     of the pass's colour parity) for the whole launch. A pass's targets in
-//     row y read rows y - 1, y and y + 1 only, so a band of n target rows
-//     needs its 2n + 1 lattice rows, which a producer warp streams in order
-//     into a ring of row slots by bulk copies (one contiguous row, plus the
-//     16-byte periodic halo at each end from the row's other end). DRAM sees
-//     long sequential reads; a band re-reads one row at each end.
+//   - A pass's targets in row y read rows y - 1, y and y + 1 only. The
+//     lattice's columns are cut into segments of at most 2048 sites, and the
+//     units of work are (segment, target row) pairs: the rows of the pass's
+//     colour parity, one segment wide. Each CTA owns a contiguous share of
+//     the units, which falls into runs of consecutive target rows of one
+//     segment; a run of n target rows needs its 2n + 1 segment rows, which a
+//     producer warp streams in order into a ring of row slots by bulk copies
+//     (the segment's contiguous stretch, plus 16 bytes of halo at each end
+//     from the neighbouring columns, wrapped at the lattice's edges). Short
+//     segment rows let the ring hold many of them, so rows land well ahead
+//     of the target rows that read them.
 //   - The consumer warps share each target row: every lane draws its
 //     targets' picks and compares the two labels, a warp queues the targets
 //     whose pick carries another label, and prices its queue in full rounds
 //     of 32, carrying fewer than 32 queued copies into its next row so the
 //     expensive path runs with every lane busy. A row slot goes back to the
-//     producer when every consumer has finished the target rows that read it
-//     (an mbarrier per slot).
-//   - The per-cell tallies a pass reads are its snapshot, complete only once
-//     every band has finished the pass before: a grid barrier (bounded, error
-//     flag 4) separates the passes' pricing. The labels a pass reads, though,
-//     changed in the pass before only on rows of that pass's parity, each in
-//     the band that priced it: a band's next rows are final once the band
-//     itself is done, except the one row at its edge that the neighbouring
-//     band owns, whose done flag the producer waits for. So a pass's rows
-//     stream in, and its light pass runs, while the grid barrier completes.
+//     producer when every consumer warp has finished the target rows that
+//     read it (an mbarrier per slot, one arrival per warp).
+//   - Passes are separated by a grid barrier (bounded, error flag 4): the
+//     per-cell tallies a pass reads are its snapshot, complete only once
+//     every CTA has finished the pass before.
 
 #include <cuda_runtime.h>
 
@@ -40,7 +39,7 @@
 namespace glz {
 
 constexpr int kBandPad = 4;         // labels of periodic halo at each end of a ring row (16 bytes)
-constexpr int kBandMaxSlots = 16;   // ring rows at most
+constexpr int kBandMaxSlots = 16;   // ring rows at most (a power of two)
 constexpr int kBandMinSlots = 8;    // five rows in use (a target row's three, the last one's two) and three ahead
 constexpr int kBandTypes = 16;      // contact tables up to 16 types live in shared memory
 constexpr long long kBandWaitLimit = 1LL << 20;     // mbarrier polls before a wait gives up
@@ -48,17 +47,10 @@ constexpr long long kBandBarrierLimit = 1LL << 22;  // grid-barrier polls (each 
 #ifndef GLZ_BAND_WARPS
 #define GLZ_BAND_WARPS 16
 #endif
-// 1: a pass's rows start streaming as soon as the band (and, for its one
-// boundary row, the neighbouring band) has finished the pass before, and only
-// the pricing waits for the grid barrier; 0: every pass waits for the whole
-// grid before its first row.
-#ifndef GLZ_BAND_OVERLAP
-#define GLZ_BAND_OVERLAP 1
+#ifndef GLZ_BAND_SEG_MAX
+#define GLZ_BAND_SEG_MAX 2048
 #endif
-constexpr bool kBandOverlap = GLZ_BAND_OVERLAP != 0;
-// The barrier words: [0] arrivals, [1] barriers completed, then per CTA the
-// passes it has completed in this launch.
-constexpr int kBandMaxGrid = 1024;
+constexpr int kBandSegMax = GLZ_BAND_SEG_MAX;  // sites of a column segment at most
 #ifndef GLZ_BAND_PER_SM
 #define GLZ_BAND_PER_SM 1
 #endif
@@ -72,6 +64,7 @@ struct BandLaunch {
     int slots;  // ring rows, a power of two
     int shift;  // log2(slots)
     int qcap;   // queue entries per consumer warp
+    int seg;    // sites of a column segment (a multiple of 4 that divides the width)
 };
 
 struct BandHead {
@@ -81,7 +74,6 @@ struct BandHead {
     float contact[kBandTypes * kBandTypes];
     int abort;   // a wait gave up: every warp stops at the pass's end
     int bar_ok;  // the grid barrier's outcome, for the whole block
-    unsigned epoch;  // passes of this launch the whole grid has completed, as this block has seen
 };
 
 __device__ __forceinline__ bool band_wait(unsigned long long *bar, uint32_t parity) {
@@ -94,23 +86,6 @@ __device__ __forceinline__ bool band_wait(unsigned long long *bar, uint32_t pari
             : "r"(b), "r"(parity)
             : "memory");
     return done != 0;
-}
-
-__device__ __forceinline__ unsigned band_load_acquire(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Wait (bounded) until the word at p reaches `want`: false if it gave up.
-// Each poll after the first few sleeps a little, so a waiting warp does not
-// take issue slots from the warps still at work.
-__device__ __forceinline__ bool band_wait_word(const unsigned *p, unsigned want) {
-    for (long long spin = 0; spin < kBandBarrierLimit; ++spin) {
-        if (band_load_acquire(p) >= want) return true;
-        if (spin >= 4) __nanosleep(64);
-    }
-    return false;
 }
 
 // The neighbour offset of pick k, decoded from compile-time constants.
@@ -148,19 +123,20 @@ __device__ __noinline__ bool band_keeps_other_colour(const SweepLaunch &a, int c
     return other != 0;
 }
 
-// Price the copy attempt at target (x, y) whose pick `pick` carries another
-// label, and commit it if the Metropolis test takes it: direct_target's
-// arithmetic (sweep.cu) operation for operation, the labels read from the
-// three ring rows rm, r0, rp (rows y - 1, y, y + 1, halo included).
+// Price the copy attempt at target (x0 + x, y) whose pick `pick` carries
+// another label, and commit it if the Metropolis test takes it:
+// direct_target's arithmetic (sweep.cu) operation for operation, the labels
+// read from the three ring rows rm, r0, rp (rows y - 1, y, y + 1 of the
+// segment starting at column x0, halo included, x counted in the segment).
 template <int NOFF, bool UNIFORM>
 __device__ __forceinline__ void band_price(const SweepLaunch &a, const BandPass &v, const float *contact,
                                            bool small_types, const uint32_t *rm, const uint32_t *r0,
-                                           const uint32_t *rp, int x, int y, int pick) {
+                                           const uint32_t *rp, int x, int x0, int y, int pick) {
     const auto at = [&](int k) -> uint32_t {
         const int dx = neighbour_offset<2, NOFF>(k, 0), dy = neighbour_offset<2, NOFF>(k, 1);
         return (dy < 0 ? rm : (dy > 0 ? rp : r0))[x + dx];
     };
-    const uint32_t target = (uint32_t)(y * a.g.w + x);
+    const uint32_t target = (uint32_t)(y * a.g.w + x0 + x);
     const uint32_t old = r0[x];
     int pdx, pdy;
     band_offset<NOFF>(pick, pdx, pdy);
@@ -267,22 +243,22 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
     const uint32_t raw = smem_addr(smem_raw);
     unsigned char *base = smem_raw + ((128u - (raw & 127u)) & 127u);
     BandHead &S = *reinterpret_cast<BandHead *>(base);
-    const int slots = B.slots, qcap = B.qcap;
+    const int slots = B.slots, qcap = B.qcap, SW = B.seg;
     const uint32_t mask = (uint32_t)slots - 1u, shift = (uint32_t)B.shift;  // slot q & mask, its use q >> shift
     uint32_t *queues = reinterpret_cast<uint32_t *>(base + ((sizeof(BandHead) + 127) / 128) * 128);
     const int W = a.g.w, H = a.g.h;
-    const int RW = W + 2 * kBandPad;
+    const int RW = SW + 2 * kBandPad;
     uint32_t *ring = queues + (((size_t)kBandWarps * qcap * 4 + 127) / 128) * 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool producer = warp == kBandWarps;
 
-    const int NT = H / 2;   // target rows a pass
-    const int HW = W / 2;   // targets a row
-    const int lo = (int)(((long long)blockIdx.x * NT) / gridDim.x);
-    const int hi = (int)(((long long)(blockIdx.x + 1) * NT) / gridDim.x);
-    const int n = hi - lo;  // this band's target rows
-    const int rows = n > 0 ? 2 * n + 1 : 0;
-    const int per_row = (HW + 32 * kBandWarps - 1) / (32 * kBandWarps);  // a lane's targets a row
+    const int NT = H / 2;                // target rows of a pass in one column segment
+    const int NS = W / SW;               // column segments
+    const long long units = (long long)NS * NT;
+    const long long lo = ((long long)blockIdx.x * units) / gridDim.x;       // this block's units:
+    const long long hi = ((long long)(blockIdx.x + 1) * units) / gridDim.x;  // (segment, target row) pairs
+    const int HSW = SW / 2;              // targets of a segment row
+    const int per_row = (HSW + 32 * kBandWarps - 1) / (32 * kBandWarps);  // a lane's targets a row
 
     if (tid == 0) {
         for (int s = 0; s < slots; ++s) {
@@ -291,7 +267,6 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
             S.last[s] = 0;
         }
         S.abort = 0;
-        S.epoch = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     const bool small_types = a.n_types <= kBandTypes;
@@ -299,7 +274,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
         for (int k = tid; k < a.n_types * a.n_types; k += blockDim.x) S.contact[k] = a.t.contact[k];
     __syncthreads();
 
-    uint32_t q0 = 0;  // ring sequence number of the pass's first row
+    uint32_t q0 = 0;  // ring sequence number of the next run's first row
     unsigned kbar = 0;
     const unsigned below = (1u << lane) - 1u;
     uint32_t *queue = queues + (size_t)(producer ? 0 : warp) * qcap;
@@ -307,229 +282,175 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
         const int32_t step = (int32_t)((uint32_t)r.step0 + (uint32_t)m);
         for (int c = 0; c < 4; ++c) {
             const long long p = r.pass0 + (long long)m * 4 + c;
-            const unsigned k = (unsigned)(m * 4 + c);  // this launch's pass number
             const int cx = c & 1, cy = (c >> 1) & 1;
-            const int cy_before = ((c + 3) >> 1) & 1;  // the parity of the rows the pass before changed
-            if (producer) {
-                if (lane == 0) {
-                    // labels the previous pass wrote (generic proxy) are read by bulk copies (async proxy)
-                    asm volatile("fence.proxy.async.global;" ::: "memory");
-                    for (int j = 0; j < rows; ++j) {
-                        if (*(volatile int *)&S.abort) break;
-                        const uint32_t q = q0 + (uint32_t)j;
-                        const int slot = (int)(q & mask);
-                        const uint32_t use = q >> shift;
-                        if (use > 0 && !band_wait(&S.empty[slot], (use - 1u) & 1u)) {
-                            atomicExch(a.error_flag, 1);
-                            S.abort = 1;
-                            break;
-                        }
-                        int yy = 2 * lo + cy - 1 + j;
-                        yy += yy < 0 ? H : (yy >= H ? -H : 0);
-                        if (kBandOverlap && k > 0 && (yy & 1) == cy_before) {
-                            // A row the pass before changed, in another band: wait for that
-                            // band to finish the pass (its labels then are final).
-                            const int tr = (yy - cy_before) / 2;
-                            const int owner = (int)(((long long)(tr + 1) * gridDim.x - 1) / NT);
-                            if (owner != (int)blockIdx.x) {
-                                if (!band_wait_word(r.barrier + 2 + owner, k)) {
-                                    atomicExch(a.error_flag, 4);
-                                    S.abort = 1;
-                                    break;
-                                }
-                                asm volatile("fence.proxy.async.global;" ::: "memory");
-                            }
-                        }
-                        const uint32_t *src = a.labels + (size_t)yy * W;
-                        uint32_t *dst = ring + (size_t)slot * RW;
-                        const uint32_t bar = smem_addr(&S.full[slot]);
-                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                                     "r"((uint32_t)(RW * 4))
-                                     : "memory");
-                        asm volatile(
-                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                                smem_addr(dst + kBandPad)),
-                            "l"(src), "r"((uint32_t)(W * 4)), "r"(bar)
-                            : "memory");
-                        asm volatile(
-                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                                smem_addr(dst)),
-                            "l"(src + W - kBandPad), "r"((uint32_t)(kBandPad * 4)), "r"(bar)
-                            : "memory");
-                        asm volatile(
-                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                                smem_addr(dst + kBandPad + W)),
-                            "l"(src), "r"((uint32_t)(kBandPad * 4)), "r"(bar)
-                            : "memory");
-                        S.last[slot] = q + 1u;
-                    }
+            const BandPass v{c, stream_key(r.seed, step, c, 1), r.vs_base[p % 2], r.vs_delta[(p + 2) % 3],
+                             reinterpret_cast<unsigned long long *>(r.vs_delta[p % 3])};
+            const uint64_t key_pick = stream_key(r.seed, step, c, 0);
+            if (!producer) {
+                // The tally rotation for the next pass, which no thread of this one reads.
+                int2 *next_base = r.vs_base[(p + 1) % 2];
+                long long *clear = r.vs_delta[(p + 1) % 3];
+                const size_t stride = (size_t)gridDim.x * kBandConsumers;
+                for (size_t l = (size_t)blockIdx.x * kBandConsumers + tid; l < (size_t)a.n_labels; l += stride) {
+                    int dv, ds;
+                    unpack_delta(v.vs_prev[l], dv, ds);
+                    const int2 b = v.vs_base[l];
+                    next_base[l] = make_int2(b.x + dv, b.y + ds);
+                    clear[l] = 0;
                 }
-            } else {
-                const BandPass v{c, stream_key(r.seed, step, c, 1), r.vs_base[p % 2], r.vs_delta[(p + 2) % 3],
-                                 reinterpret_cast<unsigned long long *>(r.vs_delta[p % 3])};
-                const uint64_t key_pick = stream_key(r.seed, step, c, 0);
-                // Before a warp prices anything in this pass, the whole grid must have
-                // finished the pass before (the tallies are its snapshot). Warp 0 polls
-                // the grid barrier and publishes what it saw in shared memory; the
-                // other warps wait on that. Then the warp does its share of the tally
-                // rotation for the next pass, which no thread of this one reads.
-                bool synced = false;
-                const auto sync_pass = [&]() -> bool {
-                    if (synced) return true;
-                    synced = true;
-                    bool ok = true;
-                    if (kBandOverlap && k > 0) {
-                        if (lane == 0) {
-                            if (warp == 0) {
-                                ok = band_wait_word(r.barrier + 1, k);
-                                if (ok)
-                                    asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(smem_addr(&S.epoch)), "r"(k)
-                                                 : "memory");
-                            } else {
-                                ok = false;
-                                for (long long spin = 0; spin < kBandBarrierLimit; ++spin) {
-                                    unsigned e;
-                                    asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(e) : "r"(smem_addr(&S.epoch))
-                                                 : "memory");
-                                    if (e >= k) {
-                                        ok = true;
-                                        break;
-                                    }
-                                    if (*(volatile int *)&S.abort) break;
-                                    __nanosleep(64);
-                                }
+            }
+            // The block's units fall into runs, one per column segment they touch:
+            // run [t0, t1) of segment `seg` streams rows 2 t0 + cy - 1 ... 2 t1 + cy - 1.
+            for (long long u0 = lo; u0 < hi;) {
+                const int seg = (int)(u0 / NT);
+                const int t0 = (int)(u0 - (long long)seg * NT);
+                const long long u1 = hi < (long long)(seg + 1) * NT ? hi : (long long)(seg + 1) * NT;
+                const int n = (int)(u1 - u0);  // target rows in this run
+                const int rows = 2 * n + 1;
+                const int x0 = seg * SW;
+                u0 = u1;
+                if (producer) {
+                    if (lane == 0) {
+                        // labels the previous pass wrote (generic proxy) are read by bulk copies (async proxy)
+                        asm volatile("fence.proxy.async.global;" ::: "memory");
+                        const int xl = x0 == 0 ? W - kBandPad : x0 - kBandPad;  // the left halo's columns
+                        const int xr = x0 + SW == W ? 0 : x0 + SW;              // the right halo's
+                        for (int j = 0; j < rows; ++j) {
+                            if (*(volatile int *)&S.abort) break;
+                            const uint32_t q = q0 + (uint32_t)j;
+                            const int slot = (int)(q & mask);
+                            const uint32_t use = q >> shift;
+                            if (use > 0 && !band_wait(&S.empty[slot], (use - 1u) & 1u)) {
+                                atomicExch(a.error_flag, 1);
+                                S.abort = 1;
+                                break;
                             }
-                            if (!ok) {
-                                atomicExch(a.error_flag, 4);
+                            int yy = 2 * t0 + cy - 1 + j;
+                            yy += yy < 0 ? H : (yy >= H ? -H : 0);
+                            const uint32_t *src = a.labels + (size_t)yy * W;
+                            uint32_t *dst = ring + (size_t)slot * RW;
+                            const uint32_t bar = smem_addr(&S.full[slot]);
+                            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                                         "r"((uint32_t)(RW * 4))
+                                         : "memory");
+                            asm volatile(
+                                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                                "[%3];" ::"r"(smem_addr(dst + kBandPad)),
+                                "l"(src + x0), "r"((uint32_t)(SW * 4)), "r"(bar)
+                                : "memory");
+                            asm volatile(
+                                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                                "[%3];" ::"r"(smem_addr(dst)),
+                                "l"(src + xl), "r"((uint32_t)(kBandPad * 4)), "r"(bar)
+                                : "memory");
+                            asm volatile(
+                                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                                "[%3];" ::"r"(smem_addr(dst + kBandPad + SW)),
+                                "l"(src + xr), "r"((uint32_t)(kBandPad * 4)), "r"(bar)
+                                : "memory");
+                            S.last[slot] = q + 1u;
+                        }
+                    }
+                } else if (!*(volatile int *)&S.abort) {
+                    const auto row_of = [&](uint32_t q) { return ring + (size_t)(q & mask) * RW + kBandPad; };
+                    const auto ready = [&](uint32_t q) { return band_wait(&S.full[q & mask], (q >> shift) & 1u); };
+                    // One arrival per warp: the warp's lanes meet first (their reads of
+                    // the slot come before lane 0's arrival), so a slot takes as many
+                    // arrivals as there are consumer warps, not threads.
+                    const auto release = [&](uint32_t q) {
+                        __syncwarp();
+                        if (lane == 0)
+                            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&S.empty[q & mask]))
+                                         : "memory");
+                    };
+                    // entries held over from the previous target row: queue[0, held), its rows and y
+                    int held = 0, hy = 0;
+                    const uint32_t *hm = nullptr, *h0 = nullptr, *hp = nullptr;
+                    bool failed = false;
+                    for (int t = 0; t < n; ++t) {
+                        const uint32_t q = q0 + 2u * (uint32_t)t + 1u;  // the target row's own ring sequence number
+                        const bool ok = (t > 0 || ready(q - 1u)) && ready(q) && ready(q + 1u);
+                        if (!__all_sync(0xffffffffu, ok) || *(volatile int *)&S.abort) {
+                            if (lane == 0 && !ok) {
+                                atomicExch(a.error_flag, 1);
                                 S.abort = 1;
                             }
-                        }
-                        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-                    }
-                    if (!ok) return false;
-                    int2 *next_base = r.vs_base[(p + 1) % 2];
-                    long long *clear = r.vs_delta[(p + 1) % 3];
-                    const size_t stride = (size_t)gridDim.x * kBandConsumers;
-                    for (size_t l = (size_t)blockIdx.x * kBandConsumers + tid; l < (size_t)a.n_labels; l += stride) {
-                        int dv, ds;
-                        unpack_delta(v.vs_prev[l], dv, ds);
-                        const int2 b = v.vs_base[l];
-                        next_base[l] = make_int2(b.x + dv, b.y + ds);
-                        clear[l] = 0;
-                    }
-                    return true;
-                };
-                if (!kBandOverlap) sync_pass();
-                const auto row_of = [&](uint32_t q) { return ring + (size_t)(q & mask) * RW + kBandPad; };
-                const auto ready = [&](uint32_t q) { return band_wait(&S.full[q & mask], (q >> shift) & 1u); };
-                // One arrival per warp: the warp's lanes meet first (their reads of
-                // the slot come before lane 0's arrival), so a slot takes as many
-                // arrivals as there are consumer warps, not threads.
-                const auto release = [&](uint32_t q) {
-                    __syncwarp();
-                    if (lane == 0)
-                        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
-                                         smem_addr(&S.empty[q & mask]))
-                                     : "memory");
-                };
-                // entries held over from the previous target row: queue[0, held), its rows and y
-                int held = 0, hy = 0;
-                const uint32_t *hm = nullptr, *h0 = nullptr, *hp = nullptr;
-                bool failed = false;
-                for (int t = 0; t < n; ++t) {
-                    const uint32_t q = q0 + 2u * (uint32_t)t + 1u;  // the target row's own ring sequence number
-                    const bool ok = (t > 0 || ready(q - 1u)) && ready(q) && ready(q + 1u);
-                    if (!__all_sync(0xffffffffu, ok) || *(volatile int *)&S.abort) {
-                        if (lane == 0 && !ok) {
-                            atomicExch(a.error_flag, 1);
-                            S.abort = 1;
-                        }
-                        failed = true;
-                        break;
-                    }
-                    const uint32_t *rm = row_of(q - 1u), *r0 = row_of(q), *rp = row_of(q + 1u);
-                    const int y = 2 * (lo + t) + cy;
-                    // Light pass: the warp's targets whose pick carries another label
-                    // join its queue behind the entries held from the previous row.
-                    int total = held;
-                    for (int part = 0; part < per_row; ++part) {
-                        const int i = (part * kBandWarps + warp) * 32 + lane;
-                        bool active = false;
-                        int pick = 0;
-                        if (i < HW) {
-                            const int x = 2 * i + cx;
-                            pick = (int)(draw(key_pick, (uint32_t)(y * W + x)) % (uint64_t)NOFF);
-                            int dx, dy;
-                            band_offset<NOFF>(pick, dx, dy);
-                            active = r0[x] != (dy < 0 ? rm : (dy > 0 ? rp : r0))[x + dx];
-                        }
-                        const unsigned mask = __ballot_sync(0xffffffffu, active);
-                        if (active) queue[total + __popc(mask & below)] = (uint32_t)i | ((uint32_t)pick << 16);
-                        total += __popc(mask);
-                    }
-                    __syncwarp();
-                    // Heavy pass: whole rounds of 32, oldest first; what is left of
-                    // the previous row goes in one last short round so its rows can
-                    // be let go; fewer than 32 of this row's stay held.
-                    int taken = 0;
-                    bool stop = false;
-                    for (;;) {
-                        const int left = total - taken;
-                        if (left < 32 && taken >= held) break;
-                        if (!sync_pass()) {
-                            stop = true;
+                            failed = true;
                             break;
                         }
-                        const int e = taken + lane;
-                        if (e < total) {
-                            const bool before = e < held;
-                            const uint32_t entry = queue[e];
-                            band_price<NOFF, UNIFORM>(a, v, S.contact, small_types, before ? hm : rm,
-                                                      before ? h0 : r0, before ? hp : rp,
-                                                      2 * (int)(entry & 0xffffu) + cx, before ? hy : y,
-                                                      (int)(entry >> 16));
+                        const uint32_t *rm = row_of(q - 1u), *r0 = row_of(q), *rp = row_of(q + 1u);
+                        const int y = 2 * (t0 + t) + cy;
+                        // Light pass: the warp's targets whose pick carries another label
+                        // join its queue behind the entries held from the previous row.
+                        int total = held;
+                        for (int part = 0; part < per_row; ++part) {
+                            const int i = (part * kBandWarps + warp) * 32 + lane;
+                            bool active = false;
+                            int pick = 0;
+                            if (i < HSW) {
+                                const int xs = 2 * i + cx;  // in the segment
+                                pick = (int)(draw(key_pick, (uint32_t)(y * W + x0 + xs)) % (uint64_t)NOFF);
+                                int dx, dy;
+                                band_offset<NOFF>(pick, dx, dy);
+                                active = r0[xs] != (dy < 0 ? rm : (dy > 0 ? rp : r0))[xs + dx];
+                            }
+                            const unsigned bits = __ballot_sync(0xffffffffu, active);
+                            if (active) queue[total + __popc(bits & below)] = (uint32_t)i | ((uint32_t)pick << 16);
+                            total += __popc(bits);
                         }
-                        taken += left < 32 ? left : 32;
-                    }
-                    __syncwarp();
-                    if (stop) {
-                        failed = true;
-                        break;
-                    }
-                    if (t > 0) {  // the previous target row (sequence q - 2) is done: its rows q - 3, q - 2
-                        release(q - 3u);
-                        release(q - 2u);
-                    }
-                    const int keep = total - taken;
-                    if (taken > 0 && keep > 0) {
-                        const uint32_t e = lane < keep ? queue[taken + lane] : 0u;
                         __syncwarp();
-                        if (lane < keep) queue[lane] = e;
+                        // Heavy pass: whole rounds of 32, oldest first; what is left of
+                        // the previous row goes in one last short round so its rows can
+                        // be let go; fewer than 32 of this row's stay held.
+                        int taken = 0;
+                        for (;;) {
+                            const int left = total - taken;
+                            if (left < 32 && taken >= held) break;
+                            const int e = taken + lane;
+                            if (e < total) {
+                                const bool before = e < held;
+                                const uint32_t entry = queue[e];
+                                band_price<NOFF, UNIFORM>(a, v, S.contact, small_types, before ? hm : rm,
+                                                          before ? h0 : r0, before ? hp : rp,
+                                                          2 * (int)(entry & 0xffffu) + cx, x0, before ? hy : y,
+                                                          (int)(entry >> 16));
+                            }
+                            taken += left < 32 ? left : 32;
+                        }
                         __syncwarp();
+                        if (t > 0) {  // the previous target row (sequence q - 2) is done: its rows q - 3, q - 2
+                            release(q - 3u);
+                            release(q - 2u);
+                        }
+                        const int keep = total - taken;
+                        if (taken > 0 && keep > 0) {
+                            const uint32_t e = lane < keep ? queue[taken + lane] : 0u;
+                            __syncwarp();
+                            if (lane < keep) queue[lane] = e;
+                            __syncwarp();
+                        }
+                        held = keep;
+                        hy = y;
+                        hm = rm;
+                        h0 = r0;
+                        hp = rp;
                     }
-                    held = keep;
-                    hy = y;
-                    hm = rm;
-                    h0 = r0;
-                    hp = rp;
-                }
-                if (n > 0 && !failed && (held == 0 || sync_pass())) {
-                    if (lane < held) {
-                        const uint32_t entry = queue[lane];
-                        band_price<NOFF, UNIFORM>(a, v, S.contact, small_types, hm, h0, hp,
-                                                  2 * (int)(entry & 0xffffu) + cx, hy, (int)(entry >> 16));
+                    if (!failed) {
+                        if (lane < held) {
+                            const uint32_t entry = queue[lane];
+                            band_price<NOFF, UNIFORM>(a, v, S.contact, small_types, hm, h0, hp,
+                                                      2 * (int)(entry & 0xffffu) + cx, x0, hy, (int)(entry >> 16));
+                        }
+                        const uint32_t ql = q0 + 2u * (uint32_t)n - 1u;  // the run's last target row
+                        release(ql - 1u);
+                        release(ql);
+                        release(ql + 1u);
                     }
-                    __syncwarp();
-                    const uint32_t ql = q0 + 2u * (uint32_t)n - 1u;  // the last target row
-                    release(ql - 1u);
-                    release(ql);
-                    release(ql + 1u);
                 }
-                if (!failed) sync_pass();  // a band that priced nothing still takes its share of the rotation
-                // this pass's label writes are read by the next pass's bulk copies
-                asm volatile("fence.proxy.async.global;" ::: "memory");
+                q0 += (uint32_t)rows;
             }
-            q0 += (uint32_t)rows;
+            // this pass's label writes are read by the next pass's bulk copies
+            asm volatile("fence.proxy.async.global;" ::: "memory");
             __syncthreads();
             if (*(volatile int *)&S.abort) {
                 // let every copy still in flight land before the block leaves
@@ -539,19 +460,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
                 __syncthreads();
                 return;
             }
-            if (kBandOverlap) {
-                // Arrive without waiting: the band's pass is done (its flag, for the
-                // neighbours' boundary rows) and the grid barrier counts it.
-                if (tid == 0) {
-                    __threadfence();
-                    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(r.barrier + 2 + blockIdx.x), "r"(k + 1u)
-                                 : "memory");
-                    if (atomicAdd(&r.barrier[0], 1u) + 1u == gridDim.x * (k + 1u)) {
-                        __threadfence();
-                        atomicExch(&r.barrier[1], k + 1u);
-                    }
-                }
-            } else if (!band_barrier(r.barrier, kbar++, &S.bar_ok)) {
+            if (!band_barrier(r.barrier, kbar++, &S.bar_ok)) {
                 if (tid == 0) atomicExch(a.error_flag, 4);
                 return;
             }
@@ -569,17 +478,25 @@ static int band_budget(int dev) {
     return share < optin ? share : optin;
 }
 
-// The launch shape of the band sweep for a plane of width w: ring rows and
-// queue room, or false when the plane does not suit it.
-static bool band_shape(int w, int h, int smem_optin, int &slots, int &shift, int &qcap, size_t &smem) {
-    if (w % 4 != 0 || w < 2 * kBandPad || h < 2 || w / 2 > 0xffff) return false;
-    const int per_row = (w / 2 + 32 * kBandWarps - 1) / (32 * kBandWarps);
+// The launch shape of the band sweep for a plane of width w: the column
+// segment (the widest that divides w, is a multiple of 4 and at most
+// kBandSegMax), ring rows (a power of two, kBandMinSlots at least) and queue
+// room; false when the plane does not suit it.
+static bool band_shape(int w, int h, int smem_budget, int &seg, int &slots, int &shift, int &qcap, size_t &smem) {
+    if (w % 4 != 0 || w < 2 * kBandPad || h < 2) return false;
+    seg = 0;
+    for (int parts = 1; parts <= w / 4; ++parts)
+        if (w % parts == 0 && (w / parts) % 4 == 0 && w / parts <= kBandSegMax) {
+            seg = w / parts;
+            break;
+        }
+    if (seg < 2 * kBandPad) return false;
+    const int per_row = (seg / 2 + 32 * kBandWarps - 1) / (32 * kBandWarps);
     qcap = 32 * per_row + 32;
     const size_t head = (sizeof(BandHead) + 127) / 128 * 128;
     const size_t queue = ((size_t)kBandWarps * qcap * 4 + 127) / 128 * 128;
-    const size_t row = (size_t)(w + 2 * kBandPad) * 4;
-    const long long room = (long long)smem_optin - 128 - (long long)head - (long long)queue;
-    if (room < (long long)row * kBandMinSlots) return false;
+    const size_t row = (size_t)(seg + 2 * kBandPad) * 4;
+    const long long room = (long long)smem_budget - 128 - (long long)head - (long long)queue;
     // the most rows that fit, rounded down to a power of two so a row's slot
     // and phase are a mask and a shift of its sequence number
     const long long fit = room / (long long)row;
@@ -606,7 +523,7 @@ static cudaError_t launch_band(const ResidentLaunch &r, cudaStream_t stream) {
     BandLaunch b{};
     b.r = r;
     size_t smem = 0;
-    if (!band_shape(r.a.g.w, r.a.g.h, optin, b.slots, b.shift, b.qcap, smem)) return cudaErrorNotSupported;
+    if (!band_shape(r.a.g.w, r.a.g.h, optin, b.seg, b.slots, b.shift, b.qcap, smem)) return cudaErrorNotSupported;
     if (cudaError_t e = cudaFuncSetAttribute(band_sweep_kernel<NOFF, UNIFORM>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))
         return e;
@@ -614,7 +531,7 @@ static cudaError_t launch_band(const ResidentLaunch &r, cudaStream_t stream) {
     if (cudaError_t e =
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, band_sweep_kernel<NOFF, UNIFORM>, kBandThreads, smem))
         return e;
-    if (per_sm < kBandPerSm || sms * kBandPerSm > kBandMaxGrid) return cudaErrorNotSupported;
+    if (per_sm < kBandPerSm) return cudaErrorNotSupported;
     void *args[] = {&b};
     return cudaLaunchCooperativeKernel((const void *)band_sweep_kernel<NOFF, UNIFORM>,
                                        dim3((unsigned)(sms * kBandPerSm)), dim3(kBandThreads), args, smem, stream);
@@ -624,9 +541,9 @@ bool band_sweep_fits(int w, int h) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return false;
     const int optin = band_budget(dev);
-    int slots = 0, shift = 0, qcap = 0;
+    int seg = 0, slots = 0, shift = 0, qcap = 0;
     size_t smem = 0;
-    return band_shape(w, h, optin, slots, shift, qcap, smem);
+    return band_shape(w, h, optin, seg, slots, shift, qcap, smem);
 }
 
 cudaError_t launch_band_sweep(const ResidentLaunch &r, cudaStream_t stream) {

@@ -790,7 +790,7 @@ int run_band(glz_gpu *h, uint64_t steps, double *ms) {
         for (int k = 0; k < 2; ++k) r.vs_base[k] = h->t.vs_base[k];
         for (int k = 0; k < 3; ++k) r.vs_delta[k] = h->t.vs_delta[k];
         r.barrier = h->barrier;
-        if (cudaMemsetAsync(h->barrier, 0, (2 + 1024) * sizeof(unsigned), h->stream) != cudaSuccess)
+        if (cudaMemsetAsync(h->barrier, 0, 2 * sizeof(unsigned), h->stream) != cudaSuccess)
             return done(fail(GLZ_DRIVER, "barrier reset failed"));
         if (ms && cudaEventRecord(ev[0], h->stream) != cudaSuccess) return done(fail(GLZ_DRIVER, "event record failed"));
         const cudaError_t e = glz::launch_band_sweep(r, h->stream);
@@ -1174,8 +1174,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     if ((rc = dev_alloc(&h->error_flag, 1))) return bail(rc);
     if ((rc = dev_alloc(&h->clock, 1))) return bail(rc);
     if (const char *graph_env = std::getenv("GLAZIER_ENGINE_GRAPH")) h->graph_on = graph_env[0] != '0';
-    // two counters, then a done flag per CTA for the band sweep
-    if ((rc = dev_alloc(&h->barrier, 2 + 1024))) return bail(rc);
+    if ((rc = dev_alloc(&h->barrier, 2))) return bail(rc);
     if ((rc = dev_alloc(&h->medium, 2))) return bail(rc);
     if ((rc = dev_alloc(&h->counters, 2))) return bail(rc);
     if (cudaMemsetAsync(h->error_flag, 0, sizeof(int), h->stream)) return bail(fail(GLZ_DRIVER, "memset failed"));
