@@ -768,7 +768,10 @@ __global__ void __launch_bounds__(kThreads, GLZ_SWEEP_MIN_BLOCKS) sweep_kernel(c
 //     (a bounded wait) before pricing. Without tensor copies (rows that are
 //     not whole 16-byte units, or a lattice smaller than a window) every cell
 //     of every window is loaded that way.
-constexpr int kLeanStages = 3;
+#ifndef GLZ_LEAN_STAGES
+#define GLZ_LEAN_STAGES 3
+#endif
+constexpr int kLeanStages = GLZ_LEAN_STAGES;
 #ifndef GLZ_LEAN_WARPS
 #define GLZ_LEAN_WARPS 8
 #endif
