@@ -135,10 +135,10 @@ def measured_peak() -> tuple:
 
 
 # DRAM bytes (read + write) of one launch of the headline sweep kernel on the
-# 4096^2 workload, from an ncu capture of that kernel (its summary is in
-# profiles/), with the kernel it was measured on. None until a capture of the
-# current kernel exists: a figure measured on another kernel is not reported.
-TRAFFIC = {"kernel": None, "bytes_per_launch": None}
+# 4096^2 workload, from an ncu capture of that kernel with cold caches
+# (profiles/lean_sweep_2d_4096.md), with the kernel it was measured on; a
+# figure measured on another kernel is not reported.
+TRAFFIC = {"kernel": "lean", "bytes_per_launch": 79988480.0}
 
 
 def ensemble_compare(mcs: int, device: int) -> dict:

@@ -7,8 +7,9 @@ replay of the schedule (oracle/replay.c) after a first MCS and at the end:
   - the plain monolayer: 128^2, 256 cells of side 8, J=10, lambda_V=1,
     V_t=64, T=10, 100 MCS;
   - the scaling sweep's planes with the surface term (lambda_S=0.2, S_t=92):
-    1024^2 and 4096^2 for 10 MCS each, the latter on the full band
-    grid, one CTA per SM, every band streaming its rows through its ring;
+    1024^2 and 4096^2 for 10 MCS each, the latter on the windowed lean
+    kernel's full persistent grid (444 CTAs walking their tiles through
+    their three-stage TMA window rings);
   - the scaling sweep's 128^3 volume, 26 neighbours, lambda_S=0.2,
     S_t=3176, for 10 MCS;
   - a lean volume just past the size from which the direct kernel queues its
@@ -68,7 +69,7 @@ def test_the_1024_plane_with_the_surface_term_replays_bit_for_bit(device):
 
 def test_the_4096_plane_with_the_surface_term_replays_bit_for_bit(device):
     start = monolayer(4096, lambda_surface=0.2, target_surface=initial_surface(8))
-    _run_both(device, start, 10, "band")
+    _run_both(device, start, 10, "lean")
 
 
 def test_the_128_volume_with_the_surface_term_replays_bit_for_bit(device):
