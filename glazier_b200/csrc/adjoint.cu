@@ -17,7 +17,8 @@
 //                   d/dd += lambda' (sum of faces of u - faces u);  d/de += -lambda' u
 // and dD = dd / k, d(decay) = de / k. The forward state is kept at every
 // `checkpoint_every`-th step; the backward recomputes each segment's sub-step
-// inputs from its checkpoint. Adjoint fields are f32; parameter gradients are
+// inputs from its checkpoint, but for the last segment, whose sub-step states
+// the forward keeps as it goes. Adjoint fields are f32; parameter gradients are
 // summed in f64 in an order fixed by the lattice alone.
 //
 // One launch runs one sub-step round of every species that has a sub-step
@@ -57,11 +58,14 @@ constexpr uint8_t kMedium = 255;
 
 struct Grid {
     int w, h, d, dim, sites;
+    glz::Divider div_w, div_h;  // w and h as multiply-shift dividers
 };
 
 __device__ __forceinline__ void faces_of(const Grid &g, size_t i, size_t nb[6]) {
     const int W = g.w, H = g.h, D = g.d;
-    const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((size_t)W * H));
+    // fewer than 2^31 sites: 32-bit quotients
+    const uint32_t r = glz::udiv(g.div_w, (uint32_t)i), pl = glz::udiv(g.div_h, r);
+    const int x = (int)((uint32_t)i - r * (uint32_t)W), y = (int)(r - pl * (uint32_t)H), z = (int)pl;
     const size_t row = ((size_t)z * H + y) * W;
     nb[0] = row + (x == 0 ? W - 1 : x - 1);
     nb[1] = row + (x == W - 1 ? 0 : x + 1);
@@ -85,6 +89,29 @@ __device__ __forceinline__ float face_sum(const Grid &g, const float *u, const s
     return sum;
 }
 
+// Every kernel here may be launched before the one ahead of it on the stream
+// has finished (programmatic dependent launch, `launch_after`): it waits for
+// that grid and its memory first, then lets the next launch start.
+__device__ __forceinline__ void grid_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class Kernel, class... Args>
+cudaError_t launch_after(Kernel kernel, int grid, size_t smem, cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 struct Species {
     const float *in;    // the sub-step's input
     float *out;         // its output (after the exchange in the last round); may be null
@@ -106,6 +133,7 @@ struct ForwardRound {
 
 // One sub-step round of the field step; the exchange on a species' last round.
 __global__ void __launch_bounds__(kThreads) forward_round(const __grid_constant__ ForwardRound a) {
+    grid_wait();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)a.g.sites) return;
     size_t nb[6];
@@ -198,15 +226,23 @@ __device__ __forceinline__ float exchange_adjoint(const BackwardRound &a, const 
 // species through its exchange (last round) and sub-step, and the gradients.
 // Each warp reduces the exchange gradients of one owner type at a time (the
 // types present in its 32 sites, in lane order of first appearance); lane 0
-// adds them to the warp's own shared row.
+// adds them to the warp's own shared row. The block's row of `partial` is
+// copied into shared memory as the launch starts, summed into there, and
+// written back at the end, so no read of it waits at the tail.
 __global__ void __launch_bounds__(kThreads) backward_round(const __grid_constant__ BackwardRound a) {
-    extern __shared__ double acc[];  // kWarps rows of 2 * n_types: sec then upt
+    grid_wait();
+    extern __shared__ double acc[];  // kWarps rows of 2 * n_types (sec then upt), then the block's n_grads row
     __shared__ double scratch[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int T = a.n_types, S = a.n_species;
     const float faces = a.g.dim == 3 ? 6.0f : 4.0f;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
-    double *row = a.partial + (size_t)blockIdx.x * a.n_grads;
+    double *global_row = a.partial + (size_t)blockIdx.x * a.n_grads;
+    double *row = acc + (size_t)kWarps * 2 * T;
+    for (int k = threadIdx.x; k < a.n_grads; k += blockDim.x)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(row + k)), "l"(global_row + k)
+                     : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
     double *mine = acc + (size_t)warp * 2 * T;
     for (int s = 0; s < S; ++s) {
         const Adjoint &p = a.sp[s];
@@ -265,7 +301,10 @@ __global__ void __launch_bounds__(kThreads) backward_round(const __grid_constant
                 }
             }
         }
-        // gradient layout: d, e per species, then sec, upt per (type, species)
+        // gradient layout: d, e per species, then sec, upt per (type, species);
+        // the row's copy has landed once every thread has waited for its own
+        // part and block_sum's barrier has passed
+        asm volatile("cp.async.wait_all;" ::: "memory");
         const double td = block_sum(gd, scratch);
         const double te = block_sum(ge, scratch);
         if (threadIdx.x == 0) {
@@ -283,16 +322,24 @@ __global__ void __launch_bounds__(kThreads) backward_round(const __grid_constant
             __syncthreads();
         }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    for (int k = threadIdx.x; k < a.n_grads; k += blockDim.x) global_row[k] = row[k];
 }
 
-// grads[k] = the sum over blocks of partial[b][k], in block order.
-__global__ void reduce_partials(const double *__restrict__ partial, int blocks, int n_grads,
-                                double *__restrict__ grads) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n_grads) return;
+// grads[k] = the sum over blocks of partial[b][k], one warp per k: lane l
+// adds rows l, l + 32, ... in order, then the warp's lanes are summed by the
+// fixed shuffle tree, so the order depends on the block count alone.
+__global__ void __launch_bounds__(kThreads) reduce_partials(const double *__restrict__ partial, int blocks, int n_grads,
+                                                            double *__restrict__ grads) {
+    grid_wait();
+    const int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (k >= n_grads) return;  // whole warps leave together
     double v = 0.0;
-    for (int b = 0; b < blocks; ++b) v += partial[(size_t)b * n_grads + k];
-    grads[k] = v;
+#pragma unroll 8
+    for (int b = lane; b < blocks; b += 32) v += partial[(size_t)b * n_grads + k];
+    v = warp_sum(v);
+    if (lane == 0) grads[k] = v;
 }
 
 // field.rs:155-160
@@ -315,7 +362,8 @@ struct glz_adj {
     float *tmp[2] = {};        // n_species * sites each: sub-step outputs inside a step
     float *work[2] = {};       // step outputs between checkpoints
     float *lam[2] = {};        // the adjoint fields
-    float *d_sec = nullptr, *d_upt = nullptr;
+    float *d_sec = nullptr, *d_upt = nullptr;  // d_sec starts the one allocation of the rate tables
+    float *staging = nullptr;                  // pinned: the rate tables on their way in
     float *d_de = nullptr;      // per-sub-step d then e per species
     float *final_out = nullptr; // n_species * sites: the forward's last step, copied to the caller
     double *partial = nullptr;  // kBlocks rows of n_grads
@@ -337,6 +385,8 @@ namespace {
 size_t field_floats(const glz_adj *h) { return (size_t)h->n_species * h->g.sites; }
 int n_grads(const glz_adj *h) { return 2 * h->n_species + 2 * h->n_types * h->n_species; }
 int blocks_for(const glz_adj *h) { return (int)((h->g.sites + kThreads - 1) / kThreads); }
+// the rate tables in one run: sec and upt per (type, species), d and e per species
+size_t table_floats(const glz_adj *h) { return (size_t)2 * h->n_types * h->n_species + 2 * h->n_species; }
 
 // The sub-step state j of species s at step `local` of the segment starting
 // at checkpoint `sg`: j < k[s] the input of sub-step j, j = k[s] the exchange
@@ -359,7 +409,10 @@ int set_params(glz_adj *h, const double *params) {
         h->k[s] = substeps(params[s], h->g.dim);
         h->kmax = h->k[s] > h->kmax ? h->k[s] : h->kmax;
     }
-    std::vector<float> sec(T * S), upt(T * S), de(2 * S);
+    // sec, upt, then d and e per species, staged in pinned memory: every
+    // forward ends in a stream synchronize, so the previous copy out of the
+    // staging has landed before it is written again
+    float *sec = h->staging, *upt = sec + T * S, *de = upt + T * S;
     for (int i = 0; i < T * S; ++i) {
         sec[i] = (float)params[2 * S + i];
         upt[i] = (float)params[2 * S + T * S + i];
@@ -368,11 +421,7 @@ int set_params(glz_adj *h, const double *params) {
         de[sp] = (float)(params[sp] / (double)h->k[sp]);
         de[S + sp] = (float)(params[S + sp] / (double)h->k[sp]);
     }
-    CU(cudaMemcpyAsync(h->d_sec, sec.data(), sec.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(h->d_upt, upt.data(), upt.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemcpyAsync(h->d_de, de.data(), de.size() * 4, cudaMemcpyHostToDevice, h->stream));
-    // the host vectors must outlive the copies
-    CU(cudaStreamSynchronize(h->stream));
+    CU(cudaMemcpyAsync(h->d_sec, h->staging, table_floats(h) * 4, cudaMemcpyHostToDevice, h->stream));
     if (h->seg_kmax != h->kmax) {
         cudaFree(h->seg);
         h->seg = nullptr;
@@ -406,42 +455,48 @@ int step_forward(glz_adj *h, int t, const float *in, float *out) {
             p.out = p.last ? out + (size_t)s * n : h->tmp[r & 1] + (size_t)s * n;
             if (p.active) cur[s] = p.out;
         }
-        forward_round<<<blocks_for(h), kThreads, 0, h->stream>>>(a);
+        CU(launch_after(forward_round, blocks_for(h), 0, h->stream, a));
     }
-    CU(cudaGetLastError());
     return GLZ_OK;
 }
 
-// Recompute segment `sg`, keeping every sub-step state; its last step's
-// output is not needed.
-int recompute(glz_adj *h, int sg, int len) {
+// Step `local` of segment `sg` forward, keeping every sub-step state in the
+// segment buffers; the output of the segment's last step goes to `last_out`
+// (not kept: null).
+int keep_step(glz_adj *h, int sg, int local, int len, float *last_out) {
     ForwardRound a{};
     a.g = h->g;
     a.n_species = h->n_species;
     a.sec = h->d_sec;
     a.upt = h->d_upt;
     a.de = h->d_de;
-    for (int local = 0; local < len; ++local) {
-        a.owner = h->owner + (size_t)(sg * h->every + local) * h->g.sites;
-        for (int r = 0; r < h->kmax; ++r) {
-            for (int s = 0; s < h->n_species; ++s) {
-                Species &p = a.sp[s];
-                p.active = r < h->k[s];
-                p.last = r == h->k[s] - 1;
-                if (!p.active) continue;
-                p.in = seg_state(h, sg, local, r, s);
-                if (p.last) {
-                    p.keep = seg_state(h, sg, local, h->k[s], s);
-                    p.out = local + 1 < len ? seg_state(h, sg, local + 1, 0, s) : nullptr;
-                } else {
-                    p.keep = nullptr;
-                    p.out = seg_state(h, sg, local, r + 1, s);
-                }
+    a.owner = h->owner + (size_t)(sg * h->every + local) * h->g.sites;
+    for (int r = 0; r < h->kmax; ++r) {
+        for (int s = 0; s < h->n_species; ++s) {
+            Species &p = a.sp[s];
+            p.active = r < h->k[s];
+            p.last = r == h->k[s] - 1;
+            if (!p.active) continue;
+            p.in = seg_state(h, sg, local, r, s);
+            if (p.last) {
+                p.keep = seg_state(h, sg, local, h->k[s], s);
+                p.out = local + 1 < len ? seg_state(h, sg, local + 1, 0, s)
+                                        : (last_out ? last_out + (size_t)s * h->g.sites : nullptr);
+            } else {
+                p.keep = nullptr;
+                p.out = seg_state(h, sg, local, r + 1, s);
             }
-            forward_round<<<blocks_for(h), kThreads, 0, h->stream>>>(a);
         }
+        CU(launch_after(forward_round, blocks_for(h), 0, h->stream, a));
     }
-    CU(cudaGetLastError());
+    return GLZ_OK;
+}
+
+// Recompute segment `sg`, keeping every sub-step state; its last step's
+// output is not needed.
+int recompute(glz_adj *h, int sg, int len) {
+    for (int local = 0; local < len; ++local)
+        if (int rc = keep_step(h, sg, local, len, nullptr)) return rc;
     return GLZ_OK;
 }
 
@@ -472,21 +527,23 @@ int capture(glz_adj *h, cudaGraphExec_t *exec, int (*body)(glz_adj *)) {
 
 // Every step forward from checkpoint 0: a step's output goes to the next
 // checkpoint, to the work buffer the step did not read, or (the last) to
-// final_out.
+// final_out. The last segment's steps keep their sub-step states as a
+// recompute would, so the backward starts without recomputing it.
 int forward_sequence(glz_adj *h) {
     const size_t n = field_floats(h);
+    const int last = (h->steps - 1) / h->every, t_last = last * h->every;
     const float *cur = h->ckpt;
-    for (int t = 0; t < h->steps; ++t) {
+    for (int t = 0; t < t_last; ++t) {
         float *dst;
-        if (t == h->steps - 1)
-            dst = h->final_out;
-        else if ((t + 1) % h->every == 0)
+        if ((t + 1) % h->every == 0)
             dst = h->ckpt + (size_t)((t + 1) / h->every) * n;
         else
             dst = cur == h->work[0] ? h->work[1] : h->work[0];
         if (int rc = step_forward(h, t, cur, dst)) return rc;
         cur = dst;
     }
+    for (int t = t_last; t < h->steps; ++t)
+        if (int rc = keep_step(h, last, t - t_last, h->steps - t_last, h->final_out)) return rc;
     return GLZ_OK;
 }
 
@@ -508,11 +565,14 @@ int backward_sequence(glz_adj *h) {
     a.upt = h->d_upt;
     a.de = h->d_de;
     a.partial = h->partial;
-    const size_t smem = (size_t)kWarps * 2 * T * sizeof(double);
+    const size_t smem = ((size_t)kWarps * 2 * T + G) * sizeof(double);
+    CU(cudaFuncSetAttribute(backward_round, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int nseg = (h->steps + h->every - 1) / h->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int t0 = sg * h->every, len = (t0 + h->every < h->steps ? t0 + h->every : h->steps) - t0;
-        if (int rc = recompute(h, sg, len)) return rc;
+        // the forward left the last segment's states in place
+        if (sg < nseg - 1)
+            if (int rc = recompute(h, sg, len)) return rc;
         for (int local = len - 1; local >= 0; --local) {
             a.owner = h->owner + (size_t)(t0 + local) * sites;
             for (int r = h->kmax - 1; r >= 0; --r) {
@@ -527,13 +587,13 @@ int backward_sequence(glz_adj *h) {
                     p.lam_in = h->lam[1 - cur[s]] + (size_t)s * sites;
                     cur[s] = 1 - cur[s];
                 }
-                backward_round<<<grid, kThreads, smem, h->stream>>>(a);
+                CU(launch_after(backward_round, grid, smem, h->stream, a));
             }
         }
         CU(cudaGetLastError());
     }
-    reduce_partials<<<(G + 127) / 128, 128, 0, h->stream>>>(h->partial, grid, G, h->d_grads);
-    CU(cudaGetLastError());
+    CU(launch_after(reduce_partials, (G + kWarps - 1) / kWarps, 0, h->stream, (const double *)h->partial, grid, G,
+                     h->d_grads));
     for (int s = 0; s < S; ++s) h->bwd_cur[s] = cur[s];
     return GLZ_OK;
 }
@@ -553,7 +613,8 @@ int glz_adj_create(int width, int height, int depth, int n_species, int n_types,
     const long long sites = (long long)width * height * depth;
     if (sites >= (1LL << 31)) return fail(GLZ_INVALID, "the lattice has 2^31 sites or more");
     glz_adj *h = new glz_adj();
-    h->g = Grid{width, height, depth, depth > 1 ? 3 : 2, (int)sites};
+    h->g = Grid{width, height, depth, depth > 1 ? 3 : 2, (int)sites, glz::make_divider((uint32_t)width),
+                glz::make_divider((uint32_t)height)};
     h->n_species = n_species;
     h->n_types = n_types;
     h->steps = steps;
@@ -573,13 +634,14 @@ int glz_adj_create(int width, int height, int depth, int n_species, int n_types,
         cudaMalloc(&h->work[1], n * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&h->lam[0], n * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&h->lam[1], n * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&h->d_sec, (size_t)n_types * n_species * 4) != cudaSuccess ||
-        cudaMalloc(&h->d_upt, (size_t)n_types * n_species * 4) != cudaSuccess ||
-        cudaMalloc(&h->d_de, (size_t)2 * n_species * 4) != cudaSuccess ||
+        cudaMalloc(&h->d_sec, table_floats(h) * 4) != cudaSuccess ||
+        cudaMallocHost(&h->staging, table_floats(h) * 4) != cudaSuccess ||
         cudaMalloc(&h->final_out, n * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&h->partial, (size_t)kBlocks * n_grads(h) * 8) != cudaSuccess ||
         cudaMalloc(&h->d_grads, (size_t)n_grads(h) * 8) != cudaSuccess)
         return bail(fail(GLZ_DRIVER, "adjoint allocation failed"));
+    h->d_upt = h->d_sec + (size_t)n_types * n_species;
+    h->d_de = h->d_upt + (size_t)n_types * n_species;
     *out = h;
     return GLZ_OK;
 }
@@ -651,7 +713,6 @@ void glz_adj_destroy(glz_adj *h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
     drop_graphs(h);
-    cudaFree(h->d_de);
     cudaFree(h->final_out);
     cudaFree(h->owner);
     cudaFree(h->ckpt);
@@ -663,7 +724,7 @@ void glz_adj_destroy(glz_adj *h) {
     cudaFree(h->lam[0]);
     cudaFree(h->lam[1]);
     cudaFree(h->d_sec);
-    cudaFree(h->d_upt);
+    cudaFreeHost(h->staging);
     cudaFree(h->partial);
     cudaFree(h->d_grads);
     if (h->stream) cudaStreamDestroy(h->stream);

@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(kBandThreads, kBandPerSm) band_sweep_kernel(co
                             int pick = 0;
                             if (i < HSW) {
                                 const int xs = 2 * i + cx;  // in the segment
-                                pick = (int)(draw(key_pick, (uint32_t)(y * W + x0 + xs)) % (uint64_t)NOFF);
+                                pick = pick_of<NOFF>(draw(key_pick, (uint32_t)(y * W + x0 + xs)));
                                 int dx, dy;
                                 band_offset<NOFF>(pick, dx, dy);
                                 active = r0[xs] != (dy < 0 ? rm : (dy > 0 ? rp : r0))[xs + dx];

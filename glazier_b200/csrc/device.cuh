@@ -19,6 +19,32 @@ constexpr uint64_t kStreamMul = 0xE7037ED1A0B428DBULL;
 // 4*colour + {0, 1} for colours 0..7.
 constexpr int kPopulationStream = 16;
 
+// Division of a 32-bit unsigned number by a divisor fixed for a launch, by a
+// high multiply and two shifts (T. Granlund, P. L. Montgomery, "Division by
+// Invariant Integers using Multiplication", PLDI 1994, section 4): with
+// l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1, the quotient of n is
+// (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0) for t = mulhi(m, n), exact
+// for every n < 2^32 and 1 <= d <= 2^31.
+struct Divider {
+    uint32_t d = 1, m = 1, s1 = 0, s2 = 0;
+};
+
+inline Divider make_divider(uint32_t d) {
+    Divider v;
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    v.d = d;
+    v.m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+    v.s1 = l < 1 ? l : 1;
+    v.s2 = l > 1 ? l - 1 : 0;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t udiv(const Divider &v, uint32_t n) {
+    const uint32_t t = __umulhi(v.m, n);
+    return (t + ((n - t) >> v.s1)) >> v.s2;
+}
+
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ULL;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
@@ -33,6 +59,21 @@ __host__ __device__ __forceinline__ uint64_t stream_key(uint64_t seed, int32_t s
 
 __host__ __device__ __forceinline__ uint64_t draw(uint64_t key, uint32_t site) {
     return mix64(key ^ (kSiteMul * (uint64_t)site));
+}
+
+// A draw reduced mod N, the neighbourhood size, fixed at compile time: a
+// power of two by its mask, any other through the 32-bit halves, as
+// ((hi mod N) (2^32 mod N) + lo mod N) mod N, which needs no 64-bit division
+// and is the same residue.
+template <int N>
+__host__ __device__ __forceinline__ int pick_of(uint64_t bits) {
+    if constexpr ((N & (N - 1)) == 0) {
+        return (int)(bits & (uint64_t)(N - 1));
+    } else {
+        constexpr uint32_t wrap32 = (uint32_t)((1ull << 32) % N);
+        const uint32_t hi = (uint32_t)(bits >> 32) % (uint32_t)N, lo = (uint32_t)bits % (uint32_t)N;
+        return (int)((hi * wrap32 + lo) % (uint32_t)N);
+    }
 }
 
 // (bits >> 11) * 2^-53 rounded to f32: the reference computes the product in

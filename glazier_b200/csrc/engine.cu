@@ -136,7 +136,7 @@ struct glz_gpu {
     bool use_tma = false;
     bool lean = false;    // the sweep prices contact, volume and surface only
     bool direct = false;  // ... on a lattice small enough for the direct kernel
-    bool compact = false; // ... queueing a warp's unlike copies (large passes)
+    int compact = 0;      // ... queueing a warp's unlike copies (1, large passes) or a block's (2)
     bool resident = false;  // ... with nothing between passes: every MCS in one launch
     bool cluster = false;   // ... a plane, in one thread-block cluster's shared memory
     bool band = false;      // ... a large plane, streamed by row bands in one launch per call
@@ -988,6 +988,7 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     g.dim = d > 1 ? 3 : 2;
     g.ncol = g.dim == 3 ? 8 : 4;
     g.sites = (int)sites;
+    glz::set_dividers(g);
     // the moment words: the geometric sums, then the nematic field's two
     h->has_nematic = nematic;
     g.nm = (g.dim == 3 ? 9 : 5) + (nematic ? 2 : 0);
@@ -1078,9 +1079,10 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     // From a million targets a pass the direct kernel queues each warp's
     // unlike copies and prices them in full rounds (GLAZIER_SWEEP_COMPACT=1:
     // at any size, =0: never).
+    // GLAZIER_SWEEP_COMPACT=2: a block-wide queue instead, at any size.
     const char *compact_env = std::getenv("GLAZIER_SWEEP_COMPACT");
-    const int compact_mode = compact_env ? (compact_env[0] == '0' ? 0 : 1) : -1;
-    h->compact = compact_mode == 1 || (compact_mode == -1 && sites / g.ncol >= glz::kDirectCompactFrom);
+    const int compact_mode = compact_env ? (compact_env[0] == '0' ? 0 : (compact_env[0] == '2' ? 2 : 1)) : -1;
+    h->compact = compact_mode >= 0 ? compact_mode : (sites / g.ncol >= glz::kDirectCompactFrom ? 1 : 0);
     // With no fields, division or death there is nothing between colour
     // passes: a direct plane of at most 512^2 sites runs every MCS of a call
     // in one cooperative launch, which saves more launch time than its grid
@@ -1392,7 +1394,7 @@ const char *glz_gpu_sweep_kernel(const glz_gpu *h) {
     if (h->band) return "band";
     if (h->cluster) return "cluster";
     if (h->resident) return "resident";
-    if (h->direct) return h->compact ? "compact" : "direct";
+    if (h->direct) return h->compact == 1 ? "compact" : (h->compact == 2 ? "gathered" : "direct");
     return h->lean ? "lean" : "general";
 }
 

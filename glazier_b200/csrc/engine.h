@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <string>
 
+#include "device.cuh"
+
 namespace glz {
 
 constexpr int kMaxSpecies = 8;
@@ -22,7 +24,17 @@ struct Geometry {
     int ring[26][3];
     uint32_t adjacency[26];
     int nm;             // exact moment sums per cell: 5 in a plane, 9 in a volume
+    // w, h and their halves (a colour's targets per row and rows per plane)
+    // as multiply-shift dividers; set_dividers fills them from w and h
+    Divider div_w, div_h, div_hw, div_hh;
 };
+
+inline void set_dividers(Geometry &g) {
+    g.div_w = make_divider((uint32_t)g.w);
+    g.div_h = make_divider((uint32_t)g.h);
+    g.div_hw = make_divider((uint32_t)(g.w / 2 > 0 ? g.w / 2 : 1));
+    g.div_hh = make_divider((uint32_t)(g.h / 2 > 0 ? g.h / 2 : 1));
+}
 
 // Per-type tables in device memory, row-major [type][...], index 0 the medium.
 struct TypeTables {
@@ -110,7 +122,7 @@ struct SweepLaunch {
     int use_tma;
     int lean;                // take the lean kernel: no length, chemotaxis, connectivity or moment tracking
     int direct;              // a lean model small enough for the direct kernel (one thread per target)
-    int compact;             // the direct kernel queues a warp's unlike copies before pricing them
+    int compact;             // the direct kernel queues unlike copies before pricing them: 1 per warp, 2 per block
     int max_ctas;            // > 0 caps the persistent grid (each CTA then walks more tiles)
     const void *tensor_map;  // CUtensorMap in device-visible memory, or null
     int *error_flag;

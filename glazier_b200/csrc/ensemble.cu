@@ -349,6 +349,7 @@ static int create_batched(int n, const glz_model *models, const uint32_t *const 
         g.ncol = g.dim == 3 ? 8 : 4;
         g.sites = w * hh * d;
         g.nm = g.dim == 3 ? 9 : 5;
+        glz::set_dividers(g);
         g.n_off = offsets_for(m.neighbour_order, d, g.off);
         if (r == 0) {
             h->dim = g.dim;

@@ -55,9 +55,11 @@ __global__ void __launch_bounds__(256) field_round_kernel(const __grid_constant_
     // with an infection rule every lane stays for the warp's dose sums
     if (!in && a.infect_species < 0) return;
     const size_t c = in ? i : 0;
-    const int x = (int)(c % W);
-    const int y = (int)((c / W) % H);
-    const int z = DIM == 3 ? (int)(c / ((size_t)W * H)) : 0;
+    // fewer than 2^31 sites: 32-bit quotients by the geometry's dividers
+    const uint32_t qw = udiv(a.g.div_w, (uint32_t)c), plane = udiv(a.g.div_h, qw);
+    const int x = (int)((uint32_t)c - qw * (uint32_t)W);
+    const int y = (int)(qw - plane * (uint32_t)H);
+    const int z = DIM == 3 ? (int)plane : 0;
     const size_t row = ((size_t)z * H + y) * W;
     const size_t xm = row + (x == 0 ? W - 1 : x - 1);
     const size_t xp = row + (x == W - 1 ? 0 : x + 1);

@@ -39,9 +39,14 @@ namespace glz {
 template <int DIM>
 struct Tile;
 
+// A plane's tile height (rows of targets and their window), a build-time knob.
+#ifndef GLZ_TILE2_TY
+#define GLZ_TILE2_TY 32
+#endif
+
 template <>
 struct Tile<2> {
-    static constexpr int TX = 128, TY = 32, TZ = 1;
+    static constexpr int TX = 128, TY = GLZ_TILE2_TY, TZ = 1;
     static constexpr int HX = 4;  // x halo rounded up to 16 bytes for the tensor copy
     static constexpr int PX = TX + 2 * HX, PY = TY + 2, PZ = 1;
     static constexpr int HZ = 0;
@@ -594,7 +599,7 @@ __device__ __forceinline__ void price_tile(const SweepLaunch &a, SweepSmem<DIM> 
         if (full || (x0 + lx < W && y0 + ly < H && (DIM == 2 || z0 + lz < D))) {
             const uint32_t target = (uint32_t)(tile_base + (lz * H + ly) * W + lx);
             const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
-            const int pick = (int)(draw(a.key_pick, target) % (uint64_t)NOFF);
+            const int pick = pick_of<NOFF>(draw(a.key_pick, target));
             active = win[wc] != win[wc + S.woff[pick]];
             entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
         }
@@ -1018,7 +1023,7 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
             bool active = false;
             int pick = 0;
             if (in) {
-                pick = (int)(draw(a.key_pick, tile_base + (uint32_t)rel[k]) % (uint64_t)NOFF);
+                pick = pick_of<NOFF>(draw(a.key_pick, tile_base + (uint32_t)rel[k]));
                 active = win[cell[k]] != win[cell[k] + S.woff[pick]];
             }
             entries[k] = (uint32_t)j | ((uint32_t)pick << 16);
@@ -1143,10 +1148,10 @@ struct GlobalPass {
 // Site (x, y, z) of target j of colour `colour` in a direct pass.
 template <int DIM>
 __device__ __forceinline__ void direct_site(const SweepLaunch &a, int colour, int j, int &x, int &y, int &z) {
-    const int hw = a.g.w / 2, hh = a.g.h / 2;
-    x = 2 * (j % hw) + (colour & 1);
-    y = 2 * ((j / hw) % hh) + ((colour >> 1) & 1);
-    z = DIM == 3 ? 2 * (j / (hw * hh)) + ((colour >> 2) & 1) : 0;
+    const uint32_t row = udiv(a.g.div_hw, (uint32_t)j), plane = udiv(a.g.div_hh, row);
+    x = 2 * (int)((uint32_t)j - row * (uint32_t)(a.g.w / 2)) + (colour & 1);
+    y = 2 * (int)(row - plane * (uint32_t)(a.g.h / 2)) + ((colour >> 1) & 1);
+    z = DIM == 3 ? 2 * (int)plane + ((colour >> 2) & 1) : 0;
 }
 
 // The connectivity veto (lib.rs:511-521) for a direct pass: the ring
@@ -1160,6 +1165,26 @@ __device__ __noinline__ bool direct_ring_one_piece(const SweepLaunch &a, int x, 
         if (a.labels[((size_t)nz * H + ny) * W + nx] == old) present |= 1u << k;
     }
     return one_piece(present, a.g.adjacency);
+}
+
+// The offset of neighbour `pick`, chosen among compile-time constants (the
+// 26-neighbourhood has a closed form) rather than read from a table.
+template <int DIM, int NOFF>
+__device__ __forceinline__ void pick_offset(int pick, int &dx, int &dy, int &dz) {
+    if constexpr (DIM == 3 && NOFF == 26) {
+        dx = neighbour_offset<3, 26>(pick, 0);
+        dy = neighbour_offset<3, 26>(pick, 1);
+        dz = neighbour_offset<3, 26>(pick, 2);
+    } else {
+        dx = dy = dz = 0;
+#pragma unroll
+        for (int k = 0; k < NOFF; ++k)
+            if (k == pick) {
+                dx = neighbour_offset<DIM, NOFF>(k, 0);
+                dy = neighbour_offset<DIM, NOFF>(k, 1);
+                dz = neighbour_offset<DIM, NOFF>(k, 2);
+            }
+    }
 }
 
 // The copy attempt at target (x, y, z) of a direct pass, its labels and
@@ -1181,11 +1206,11 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access
         return acc.label(nx, ny, nz);
     };
     const uint32_t target = (uint32_t)((z * H + y) * W + x);
-    const int pick = known_pick >= 0 ? known_pick : (int)(draw(key_pick, target) % (uint64_t)NOFF);
-    uint32_t nw = 0;
-#pragma unroll
-    for (int k = 0; k < NOFF; ++k)
-        if (k == pick) nw = at(k);
+    const int pick = known_pick >= 0 ? known_pick : pick_of<NOFF>(draw(key_pick, target));
+    int dx, dy, dz;
+    pick_offset<DIM, NOFF>(pick, dx, dy, dz);
+    const uint32_t nw = acc.label(dx < 0 ? xm : (dx > 0 ? xp : x), dy < 0 ? ym : (dy > 0 ? yp : y),
+                                  dz < 0 ? zm : (dz > 0 ? zp : z));
     const uint32_t old = acc.label(x, y, z);
     if (old == nw) return;
     const int2 base_old = acc.base(old), base_new = acc.base(nw);
@@ -1243,26 +1268,6 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access
     if (EXTRAS && a.tracks) commit_moments<DIM>(a, old, nw, x, y, z);
 }
 
-// The offset of neighbour `pick`, chosen among compile-time constants (the
-// 26-neighbourhood has a closed form) rather than read from a table.
-template <int DIM, int NOFF>
-__device__ __forceinline__ void pick_offset(int pick, int &dx, int &dy, int &dz) {
-    if constexpr (DIM == 3 && NOFF == 26) {
-        dx = neighbour_offset<3, 26>(pick, 0);
-        dy = neighbour_offset<3, 26>(pick, 1);
-        dz = neighbour_offset<3, 26>(pick, 2);
-    } else {
-        dx = dy = dz = 0;
-#pragma unroll
-        for (int k = 0; k < NOFF; ++k)
-            if (k == pick) {
-                dx = neighbour_offset<DIM, NOFF>(k, 0);
-                dy = neighbour_offset<DIM, NOFF>(k, 1);
-                dz = neighbour_offset<DIM, NOFF>(k, 2);
-            }
-    }
-}
-
 // K 0: one target per thread, priced where it lies. K > 0: each warp takes
 // 32 K consecutive targets; every lane draws its targets' picks and compares
 // the two labels, the targets whose pick carries another label go into the
@@ -1272,6 +1277,14 @@ __device__ __forceinline__ void pick_offset(int pick, int &dx, int &dy, int &dz)
 // a pass (kDirectCompactFrom, engine.h) the plain form's four times wider
 // grid hides more latency and is as fast or faster.
 constexpr int kDirectCompactK = 4;
+// K < 0: the block's 256 |K| consecutive targets are drawn and compared by
+// all its threads, the unlike ones gathered into one block-wide queue, and
+// the queue priced from its front by as many whole warps as it needs: the
+// plain form's wide grid, with a warp's lanes busy in the pricing rounds.
+#ifndef GLZ_DIRECT_BLOCK_K
+#define GLZ_DIRECT_BLOCK_K 1
+#endif
+constexpr int kDirectBlockK = -GLZ_DIRECT_BLOCK_K;
 
 template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
 __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
@@ -1284,6 +1297,59 @@ __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
             int x, y, z;
             direct_site<DIM>(a, a.colour, j, x, y, z);
             direct_target<DIM, NOFF, UNIFORM, GlobalPass, EXTRAS>(a, acc, v.key_pick, v.key_accept, x, y, z);
+        }
+    } else if constexpr (K < 0) {
+        constexpr int KB = -K;
+        __shared__ int queue[256 * KB];
+        __shared__ uint8_t picks[256 * KB];
+        __shared__ int counts[8];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const unsigned below = (1u << lane) - 1u;
+        const int first = blockIdx.x * 256 * KB;
+        unsigned masks[KB];
+        int picked[KB];
+        int mine = 0;
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            const int j = first + k * 256 + (int)threadIdx.x;
+            bool unlike = false;
+            int pick = 0;
+            if (j < targets) {
+                int x, y, z;
+                direct_site<DIM>(a, a.colour, j, x, y, z);
+                pick = pick_of<NOFF>(draw(v.key_pick, (uint32_t)((z * a.g.h + y) * a.g.w + x)));
+                int dx, dy, dz;
+                pick_offset<DIM, NOFF>(pick, dx, dy, dz);
+                const int nx = x + dx < 0 ? a.g.w - 1 : (x + dx >= a.g.w ? 0 : x + dx);
+                const int ny = y + dy < 0 ? a.g.h - 1 : (y + dy >= a.g.h ? 0 : y + dy);
+                const int nz = z + dz < 0 ? a.g.d - 1 : (z + dz >= a.g.d ? 0 : z + dz);
+                unlike = acc.label(x, y, z) != acc.label(nx, ny, nz);
+            }
+            masks[k] = __ballot_sync(0xffffffffu, unlike);
+            picked[k] = pick;
+            mine += __popc(masks[k]);
+        }
+        if (lane == 0) counts[warp] = mine;
+        __syncthreads();
+        int at = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            at += w < warp ? counts[w] : 0;
+            total += counts[w];
+        }
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            if (masks[k] & (1u << lane)) {
+                queue[at + __popc(masks[k] & below)] = first + k * 256 + (int)threadIdx.x;
+                picks[at + __popc(masks[k] & below)] = (uint8_t)picked[k];
+            }
+            at += __popc(masks[k]);
+        }
+        __syncthreads();
+        for (int e = (int)threadIdx.x; e < total; e += 256) {
+            int x, y, z;
+            direct_site<DIM>(a, a.colour, queue[e], x, y, z);
+            direct_target<DIM, NOFF, UNIFORM, GlobalPass, EXTRAS>(a, acc, v.key_pick, v.key_accept, x, y, z, picks[e]);
         }
     } else {
         __shared__ int queue[8][32 * K];
@@ -1300,7 +1366,7 @@ __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
             if (j < targets) {
                 int x, y, z;
                 direct_site<DIM>(a, a.colour, j, x, y, z);
-                pick = (int)(draw(v.key_pick, (uint32_t)((z * a.g.h + y) * a.g.w + x)) % (uint64_t)NOFF);
+                pick = pick_of<NOFF>(draw(v.key_pick, (uint32_t)((z * a.g.h + y) * a.g.w + x)));
                 int dx, dy, dz;
                 pick_offset<DIM, NOFF>(pick, dx, dy, dz);
                 const int nx = x + dx < 0 ? a.g.w - 1 : (x + dx >= a.g.w ? 0 : x + dx);
@@ -1719,8 +1785,8 @@ static int programmatic_launch() {
 template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
     const int targets = (a.g.w / 2) * (a.g.h / 2) * (DIM == 3 ? a.g.d / 2 : 1);
-    const bool compact = a.compact != 0;
-    const int per_block = 256 * (compact ? kDirectCompactK : 1);
+    const bool compact = a.compact == 1, gathered = a.compact == 2;
+    const int per_block = 256 * (compact ? kDirectCompactK : (gathered ? -kDirectBlockK : 1));
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)((targets + per_block - 1) / per_block));
     cfg.blockDim = dim3(256);
@@ -1734,17 +1800,20 @@ static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
     if (a.clock) {  // a step captured into a graph: plain launches, pass fields from the clock
         cfg.numAttrs = 0;
         if (!a.lean)
-            return compact
-                       ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
-                       : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, true>, a);
-        return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
-                       : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, false>, a);
+            return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
+                   : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK, true>, a)
+                              : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, true>, a);
+        return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
+               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK, false>, a)
+                          : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, false>, a);
     }
     if (!a.lean)  // every term: length, chemotaxis, connectivity, motility, drift, nematic, moments
-        return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
-                       : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, true>, a);
-    return compact ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
-                   : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, false>, a);
+        return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
+               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK, true>, a)
+                          : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, true>, a);
+    return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
+           : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK, false>, a)
+                      : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, false>, a);
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
@@ -2185,7 +2254,7 @@ __global__ void __launch_bounds__(kLeanThreads, GLZ_LEAN_MIN_BLOCKS)
             int pick = 0;
             if (in) {
                 const int wc = ((lz + T::HZ) * T::PY + (ly + 1)) * T::PX + (lx + T::HX);
-                pick = (int)(draw(a.key_pick, tile_base + (uint32_t)((lz * H + ly) * W + lx)) % (uint64_t)NOFF);
+                pick = pick_of<NOFF>(draw(a.key_pick, tile_base + (uint32_t)((lz * H + ly) * W + lx)));
                 active = win[wc] != win[wc + S.woff[pick]];
             }
             entries[k] = (uint32_t)j | ((uint32_t)pick << 16);

@@ -18,11 +18,12 @@ namespace glz {
 
 // A lattice holds fewer than 2^31 sites, so 32-bit division suffices.
 __device__ __forceinline__ void coords_of(const Geometry &g, size_t i, int &x, int &y, int &z) {
-    const uint32_t s = (uint32_t)i, w = (uint32_t)g.w, h = (uint32_t)g.h;
-    const uint32_t row = s / w;
-    x = (int)(s - row * w);
-    y = (int)(row % h);
-    z = (int)(row / h);
+    const uint32_t s = (uint32_t)i;
+    const uint32_t row = udiv(g.div_w, s);
+    const uint32_t plane = udiv(g.div_h, row);
+    x = (int)(s - row * (uint32_t)g.w);
+    y = (int)(row - plane * (uint32_t)g.h);
+    z = (int)plane;
 }
 
 // The label count a recount covers: the live count in device memory for a

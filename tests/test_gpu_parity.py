@@ -190,7 +190,7 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("kernel", ["band", "cluster", "resident", "direct", "compact", "lean", "general"])
+@pytest.mark.parametrize("kernel", ["band", "cluster", "resident", "direct", "compact", "gathered", "lean", "general"])
 @pytest.mark.parametrize("ctas", ["0", "3"])
 @pytest.mark.parametrize("tma", ["1", "0"])
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -202,17 +202,18 @@ def test_the_device_reproduces_the_replay_bit_for_bit(device, name, tma, ctas, k
     cluster's shared memory), the resident (every MCS of a call in one
     launch, for models with nothing between passes), the direct (one thread a
     target, or with `compact` each warp's unlike copies queued and priced in
-    full rounds), the lean or the general kernel (models with other terms
+    full rounds, or with `gathered` a block's), the lean or the general kernel (models with other terms
     always take the general one)."""
-    if kernel in ("band", "cluster", "resident", "direct", "compact") and (tma == "0" or ctas == "3"):
+    if kernel in ("band", "cluster", "resident", "direct", "compact", "gathered") and (tma == "0" or ctas == "3"):
         pytest.skip("the band, resident and direct kernels take no tensor copies and no grid cap")
     made, steps = CASES[name]()
     start, fields = made if isinstance(made, tuple) else (made, None)
     monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
     monkeypatch.setenv("GLAZIER_SWEEP_CTAS", ctas)
     monkeypatch.setenv("GLAZIER_SWEEP_LEAN", "0" if kernel == "general" else "1")
-    monkeypatch.setenv("GLAZIER_SWEEP_DIRECT", "1" if kernel in ("cluster", "resident", "direct", "compact") else "0")
-    monkeypatch.setenv("GLAZIER_SWEEP_COMPACT", "1" if kernel == "compact" else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_DIRECT",
+                       "1" if kernel in ("cluster", "resident", "direct", "compact", "gathered") else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_COMPACT", {"compact": "1", "gathered": "2"}.get(kernel, "0"))
     monkeypatch.setenv("GLAZIER_SWEEP_RESIDENT", "1" if kernel in ("cluster", "resident") else "0")
     monkeypatch.setenv("GLAZIER_SWEEP_CLUSTER", "1" if kernel == "cluster" else "0")
     monkeypatch.setenv("GLAZIER_SWEEP_BAND", "1" if kernel == "band" else "0")

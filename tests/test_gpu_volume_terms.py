@@ -11,7 +11,7 @@ bit-exact parity with the host replay of the schedule.
   sub-steps, the veto over the 26 ring, death, motile immune cells climbing
   the virus), against the replay: labels, volumes, surfaces, cell types and
   the f32 field identical after the first MCS and after 12, on the direct
-  kernel (plain and queued) and on the tiled general kernel with the window's
+  kernel (plain, warp-queued and block-queued) and on the tiled general kernel with the window's
   tensor copy on and off and the persistent grid at its default and capped at
   three CTAs.
 - Division in a volume: cells that grow past their division volume are cut
@@ -84,11 +84,11 @@ CASES = {"every-term": _every_term, "infection-volume": _infection_volume, "divi
 
 
 # (kernel, tensor copies, persistent grid cap): the direct kernel (one thread
-# per target, the default for these sizes), its queued form, and the tiled
-# general kernel with its window copied by TMA or by plain loads, its grid at
-# the default or capped at three CTAs
-MODES = {"direct": ("direct", "1", "0"), "compact": ("compact", "1", "0"), "tiled": ("general", "1", "0"),
-         "tiled-plain": ("general", "0", "0"), "tiled-capped": ("general", "1", "3")}
+# per target, the default for these sizes), its warp- and block-queued forms,
+# and the tiled general kernel with its window copied by TMA or by plain
+# loads, its grid at the default or capped at three CTAs
+MODES = {"direct": ("direct", "1", "0"), "compact": ("compact", "1", "0"), "gathered": ("gathered", "1", "0"),
+         "tiled": ("general", "1", "0"), "tiled-plain": ("general", "0", "0"), "tiled-capped": ("general", "1", "3")}
 
 
 @pytest.mark.parametrize("mode", sorted(MODES))
@@ -98,7 +98,7 @@ def test_a_volume_with_every_term_reproduces_the_replay_bit_for_bit(device, name
     monkeypatch.setenv("GLAZIER_SWEEP_TMA", tma)
     monkeypatch.setenv("GLAZIER_SWEEP_CTAS", ctas)
     monkeypatch.setenv("GLAZIER_SWEEP_DIRECT", "0" if kernel == "general" else "1")
-    monkeypatch.setenv("GLAZIER_SWEEP_COMPACT", "1" if kernel == "compact" else "0")
+    monkeypatch.setenv("GLAZIER_SWEEP_COMPACT", {"compact": "1", "gathered": "2"}.get(kernel, "0"))
     start = CASES[name]()
     gpu = device.GpuSimulation.from_start(start)
     assert gpu.sweep_kernel == kernel
