@@ -160,6 +160,117 @@ __global__ void __launch_bounds__(kThreads) forward_round(const __grid_constant_
     }
 }
 
+// Lattices whose rows are whole multiples of four sites take the round
+// kernels in four-site form: a thread takes sites x0 .. x0 + 3 of a row (x0
+// a multiple of 4), reads the row and the rows across its y (and z) faces as
+// float4 and the two x neighbours past its ends as scalars, so neighbouring
+// sites share their loads. Each site's arithmetic is the one-site kernel's,
+// operation for operation, so both forms give the same field bits.
+struct Quad {
+    size_t c;     // the first of the four sites
+    size_t l, r;  // the x neighbour before the first and after the last
+    size_t f[4];  // the same four x in the rows across the y-1, y+1, z-1 and z+1 faces
+};
+
+__device__ __forceinline__ Quad quad_of(const Grid &g, size_t q) {
+    const int W = g.w, H = g.h, D = g.d;
+    const uint32_t i = (uint32_t)(4 * q);  // fewer than 2^31 sites
+    const uint32_t rw = glz::udiv(g.div_w, i), pl = glz::udiv(g.div_h, rw);
+    const int x0 = (int)(i - rw * (uint32_t)W), y = (int)(rw - pl * (uint32_t)H), z = (int)pl;
+    const size_t row = ((size_t)z * H + y) * W;
+    Quad o;
+    o.c = row + x0;
+    o.l = row + (x0 == 0 ? W - 1 : x0 - 1);
+    o.r = row + (x0 + 4 == W ? 0 : x0 + 4);
+    o.f[0] = ((size_t)z * H + (y == 0 ? H - 1 : y - 1)) * W + x0;
+    o.f[1] = ((size_t)z * H + (y == H - 1 ? 0 : y + 1)) * W + x0;
+    o.f[2] = g.dim == 3 ? ((size_t)(z == 0 ? D - 1 : z - 1) * H + y) * W + x0 : 0;
+    o.f[3] = g.dim == 3 ? ((size_t)(z == D - 1 ? 0 : z + 1) * H + y) * W + x0 : 0;
+    return o;
+}
+
+__device__ __forceinline__ void ld4(const float *p, float v[4]) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+}
+
+__device__ __forceinline__ void st4(float *p, const float v[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+__device__ __forceinline__ void ld4(const uint8_t *p, int v[4]) {
+    const uchar4 t = *reinterpret_cast<const uchar4 *>(p);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+}
+
+// The four sites' face sums, in face_sum's order, from their own values h,
+// the x neighbours past the ends xl and xr, and the rows across the faces.
+__device__ __forceinline__ void quad_sums(bool volume, const float h[4], float xl, float xr, const float fy0[4],
+                                          const float fy1[4], const float fz0[4], const float fz1[4], float sum[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float v = __fadd_rn(k == 0 ? xl : h[k - 1], k == 3 ? xr : h[k + 1]);
+        v = __fadd_rn(v, fy0[k]);
+        v = __fadd_rn(v, fy1[k]);
+        if (volume) {
+            v = __fadd_rn(v, fz0[k]);
+            v = __fadd_rn(v, fz1[k]);
+        }
+        sum[k] = v;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) forward_quads(const __grid_constant__ ForwardRound a) {
+    grid_wait();
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)a.g.sites / 4) return;
+    const Quad o = quad_of(a.g, q);
+    const bool volume = a.g.dim == 3;
+    const float faces = volume ? 6.0f : 4.0f;
+    int own[4];
+    bool have_own = false;
+    for (int s = 0; s < a.n_species; ++s) {
+        const Species &p = a.sp[s];
+        if (!p.active) continue;
+        float h[4], fy0[4], fy1[4], fz0[4] = {}, fz1[4] = {}, sum[4], v[4];
+        ld4(p.in + o.c, h);
+        ld4(p.in + o.f[0], fy0);
+        ld4(p.in + o.f[1], fy1);
+        if (volume) {
+            ld4(p.in + o.f[2], fz0);
+            ld4(p.in + o.f[3], fz1);
+        }
+        quad_sums(volume, h, p.in[o.l], p.in[o.r], fy0, fy1, fz0, fz1, sum);
+        const float d = a.de[s], e = a.de[a.n_species + s];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            v[k] = __fsub_rn(__fadd_rn(h[k], __fmul_rn(d, __fsub_rn(sum[k], __fmul_rn(faces, h[k])))), __fmul_rn(e, h[k]));
+        if (p.last) {
+            if (p.keep) st4(p.keep + o.c, v);
+            if (!have_own) {
+                ld4(a.owner + o.c, own);
+                have_own = true;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int t = own[k];
+                if (t != kMedium) {
+                    v[k] = __fadd_rn(v[k], a.sec[t * a.n_species + s]);
+                    v[k] = __fsub_rn(v[k], __fmul_rn(a.upt[t * a.n_species + s], v[k]));
+                    v[k] = v[k] < 0.0f ? 0.0f : v[k];
+                }
+            }
+        }
+        if (p.out) st4(p.out + o.c, v);
+    }
+}
+
 // Parameter gradients are summed without atomics, in an order fixed by the
 // lattice alone, so a backward is bit-reproducible and independent of the
 // checkpoint interval: the backward kernel runs on a fixed grid of at most
@@ -327,6 +438,230 @@ __global__ void __launch_bounds__(kThreads) backward_round(const __grid_constant
     for (int k = threadIdx.x; k < a.n_grads; k += blockDim.x) global_row[k] = row[k];
 }
 
+// A species' rates for owner type t: from registers holding the first TMAX
+// types (TMAX > 0, every type below TMAX), else from the tables.
+template <int TMAX>
+struct Rates {
+    float sec[TMAX > 0 ? TMAX : 1], upt[TMAX > 0 ? TMAX : 1];
+    const float *gsec, *gupt;  // the tables at the species, stride n_species
+    int stride;
+    __device__ __forceinline__ void load(const float *sec_table, const float *upt_table, int s, int n_species,
+                                         int n_types) {
+        gsec = sec_table + s;
+        gupt = upt_table + s;
+        stride = n_species;
+#pragma unroll
+        for (int tt = 0; tt < (TMAX > 0 ? TMAX : 1); ++tt) {
+            sec[tt] = TMAX > 0 && tt < n_types ? gsec[tt * stride] : 0.0f;
+            upt[tt] = TMAX > 0 && tt < n_types ? gupt[tt * stride] : 0.0f;
+        }
+    }
+    __device__ __forceinline__ void of(int t, float &s_out, float &u_out) const {
+        if (TMAX > 0) {
+            s_out = sec[0];
+            u_out = upt[0];
+#pragma unroll
+            for (int tt = 1; tt < (TMAX > 0 ? TMAX : 1); ++tt)
+                if (t == tt) {
+                    s_out = sec[tt];
+                    u_out = upt[tt];
+                }
+        } else {
+            s_out = gsec[t * stride];
+            u_out = gupt[t * stride];
+        }
+    }
+};
+
+// The exchange adjoint of one site of type t (kMedium: none) whose exchange
+// input was x: exchange_adjoint with the owner, the input and the rates
+// already read.
+template <int TMAX>
+__device__ __forceinline__ float exchange_adjoint_at(const Rates<TMAX> &r, int t, float x, float l, float *v1_out,
+                                                     float *lv_out) {
+    if (t == kMedium) return l;
+    float sec, q;
+    r.of(t, sec, q);
+    const float v1 = __fadd_rn(x, sec);
+    const float v2 = __fsub_rn(v1, __fmul_rn(q, v1));
+    const float lv = v2 < 0.0f ? 0.0f : l;
+    *v1_out = v1;
+    *lv_out = lv;
+    return __fmul_rn(lv, __fsub_rn(1.0f, q));
+}
+
+// backward_round in four-site form. Each thread adds its four sites'
+// gradient terms in x order. With TMAX > 0 (every owner type below TMAX)
+// each thread also keeps its exchange gradients per owner type in registers
+// across its trips, and each warp sums them once at the end of a species;
+// with TMAX 0 the warps reduce them type by type on every trip, as
+// backward_round does. Either way the order is fixed by the lattice.
+template <int TMAX>
+__global__ void __launch_bounds__(kThreads) backward_quads(const __grid_constant__ BackwardRound a) {
+    grid_wait();
+    extern __shared__ double acc[];  // kWarps rows of 2 * n_types (sec then upt), then the block's n_grads row
+    __shared__ double scratch[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int T = a.n_types, S = a.n_species;
+    const bool volume = a.g.dim == 3;
+    const float faces = volume ? 6.0f : 4.0f;
+    const size_t quads = (size_t)a.g.sites / 4, stride = (size_t)gridDim.x * blockDim.x;
+    double *global_row = a.partial + (size_t)blockIdx.x * a.n_grads;
+    double *row = acc + (size_t)kWarps * 2 * T;
+    for (int k = threadIdx.x; k < a.n_grads; k += blockDim.x)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(row + k)),
+                     "l"(global_row + k)
+                     : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    double *mine = acc + (size_t)warp * 2 * T;
+    for (int s = 0; s < S; ++s) {
+        const Adjoint &p = a.sp[s];
+        if (!p.active) continue;
+        if (p.last) {
+            for (int k = threadIdx.x; k < kWarps * 2 * T; k += blockDim.x) acc[k] = 0.0;
+            __syncthreads();
+        }
+        double gd = 0.0, ge = 0.0;
+        double tsec[TMAX > 0 ? TMAX : 1] = {}, tupt[TMAX > 0 ? TMAX : 1] = {};  // per owner type, TMAX > 0
+        const float d = a.de[s], e = a.de[S + s];
+        Rates<TMAX> rates;
+        rates.load(a.sec, a.upt, s, S, T);
+        // every lane of a warp takes the same number of trips
+        for (size_t base = (size_t)blockIdx.x * blockDim.x; base < quads; base += stride) {
+            const size_t q = base + threadIdx.x;
+            const bool in = q < quads;
+            float l1[4] = {}, dupt[4] = {};
+            int t[4] = {kMedium, kMedium, kMedium, kMedium};
+            if (in) {
+                const Quad o = quad_of(a.g, q);
+                float l[4], fy0[4], fy1[4], fz0[4] = {}, fz1[4] = {}, ls[4];
+                ld4(p.lam + o.c, l);
+                ld4(p.lam + o.f[0], fy0);
+                ld4(p.lam + o.f[1], fy1);
+                if (volume) {
+                    ld4(p.lam + o.f[2], fz0);
+                    ld4(p.lam + o.f[3], fz1);
+                }
+                float xl = p.lam[o.l], xr = p.lam[o.r];
+                // the sub-step input, read before anything is written
+                float u[4], uy0[4], uy1[4], uz0[4] = {}, uz1[4] = {}, us[4];
+                ld4(p.u + o.c, u);
+                ld4(p.u + o.f[0], uy0);
+                ld4(p.u + o.f[1], uy1);
+                if (volume) {
+                    ld4(p.u + o.f[2], uz0);
+                    ld4(p.u + o.f[3], uz1);
+                }
+                const float ul = p.u[o.l], ur = p.u[o.r];
+                if (p.last) {
+                    float x[4], v1, lv;
+                    ld4(a.owner + o.c, t);
+                    ld4(p.exch + o.c, x);
+                    int ty0[4], ty1[4], tz0[4] = {}, tz1[4] = {};
+                    float xy0[4], xy1[4], xz0[4] = {}, xz1[4] = {};
+                    ld4(a.owner + o.f[0], ty0);
+                    ld4(p.exch + o.f[0], xy0);
+                    ld4(a.owner + o.f[1], ty1);
+                    ld4(p.exch + o.f[1], xy1);
+                    if (volume) {
+                        ld4(a.owner + o.f[2], tz0);
+                        ld4(p.exch + o.f[2], xz0);
+                        ld4(a.owner + o.f[3], tz1);
+                        ld4(p.exch + o.f[3], xz1);
+                    }
+                    const int tl = a.owner[o.l], tr = a.owner[o.r];
+                    const float xxl = p.exch[o.l], xxr = p.exch[o.r];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        l[k] = exchange_adjoint_at(rates, t[k], x[k], l[k], &v1, &lv);
+                        if (t[k] != kMedium) {
+                            l1[k] = l[k];
+                            dupt[k] = -__fmul_rn(lv, v1);
+                        }
+                        fy0[k] = exchange_adjoint_at(rates, ty0[k], xy0[k], fy0[k], &v1, &lv);
+                        fy1[k] = exchange_adjoint_at(rates, ty1[k], xy1[k], fy1[k], &v1, &lv);
+                        if (volume) {
+                            fz0[k] = exchange_adjoint_at(rates, tz0[k], xz0[k], fz0[k], &v1, &lv);
+                            fz1[k] = exchange_adjoint_at(rates, tz1[k], xz1[k], fz1[k], &v1, &lv);
+                        }
+                    }
+                    xl = exchange_adjoint_at(rates, tl, xxl, xl, &v1, &lv);
+                    xr = exchange_adjoint_at(rates, tr, xxr, xr, &v1, &lv);
+                }
+                quad_sums(volume, l, xl, xr, fy0, fy1, fz0, fz1, ls);
+                float li[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    li[k] = __fsub_rn(__fadd_rn(l[k], __fmul_rn(d, __fsub_rn(ls[k], __fmul_rn(faces, l[k])))),
+                                      __fmul_rn(e, l[k]));
+                st4(p.lam_in + o.c, li);
+                quad_sums(volume, u, ul, ur, uy0, uy1, uz0, uz1, us);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    gd += (double)__fmul_rn(l[k], __fsub_rn(us[k], __fmul_rn(faces, u[k])));
+                    ge -= (double)__fmul_rn(l[k], u[k]);
+                }
+            }
+            if (TMAX > 0 && p.last) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+#pragma unroll
+                    for (int tt = 0; tt < (TMAX > 0 ? TMAX : 1); ++tt) {
+                        tsec[tt] += t[k] == tt ? (double)l1[k] : 0.0;
+                        tupt[tt] += t[k] == tt ? (double)dupt[k] : 0.0;
+                    }
+            } else if (p.last) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    unsigned todo = __ballot_sync(0xffffffffu, t[k] != kMedium);
+                    while (todo) {
+                        const int leader = __ffs(todo) - 1;
+                        const int tt = __shfl_sync(0xffffffffu, t[k], leader);
+                        const bool same = t[k] == tt;
+                        const double x = warp_sum(same ? (double)l1[k] : 0.0);
+                        const double y = warp_sum(same ? (double)dupt[k] : 0.0);
+                        if (lane == 0) {
+                            mine[tt] += x;
+                            mine[T + tt] += y;
+                        }
+                        todo &= ~__ballot_sync(0xffffffffu, same);
+                    }
+                }
+            }
+        }
+        if (TMAX > 0 && p.last) {
+#pragma unroll
+            for (int tt = 0; tt < (TMAX > 0 ? TMAX : 1); ++tt) {
+                const double x = warp_sum(tsec[tt]), y = warp_sum(tupt[tt]);
+                if (lane == 0 && tt < T) {
+                    mine[tt] = x;
+                    mine[T + tt] = y;
+                }
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        const double td = block_sum(gd, scratch);
+        const double te = block_sum(ge, scratch);
+        if (threadIdx.x == 0) {
+            row[s] += td;
+            row[S + s] += te;
+        }
+        if (p.last) {
+            __syncthreads();
+            for (int k = threadIdx.x; k < 2 * T; k += blockDim.x) {
+                double v = 0.0;
+                for (int w = 0; w < kWarps; ++w) v += acc[(size_t)w * 2 * T + k];
+                const int tt = k % T;
+                row[(k < T ? 2 * S : 2 * S + T * S) + tt * S + s] += v;
+            }
+            __syncthreads();
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    for (int k = threadIdx.x; k < a.n_grads; k += blockDim.x) global_row[k] = row[k];
+}
+
 // grads[k] = the sum over blocks of partial[b][k], one warp per k: lane l
 // adds rows l, l + 32, ... in order, then the warp's lanes are summed by the
 // fixed shuffle tree, so the order depends on the block count alone.
@@ -384,7 +719,18 @@ namespace {
 
 size_t field_floats(const glz_adj *h) { return (size_t)h->n_species * h->g.sites; }
 int n_grads(const glz_adj *h) { return 2 * h->n_species + 2 * h->n_types * h->n_species; }
-int blocks_for(const glz_adj *h) { return (int)((h->g.sites + kThreads - 1) / kThreads); }
+// Rows of whole multiples of four sites take the four-site kernels.
+bool quads(const glz_adj *h) { return h->g.w % 4 == 0; }
+int blocks_for(const glz_adj *h) {
+    const long long items = quads(h) ? h->g.sites / 4 : h->g.sites;
+    return (int)((items + kThreads - 1) / kThreads);
+}
+
+int launch_forward(glz_adj *h, const ForwardRound &a) {
+    CU(quads(h) ? launch_after(forward_quads, blocks_for(h), 0, h->stream, a)
+                : launch_after(forward_round, blocks_for(h), 0, h->stream, a));
+    return GLZ_OK;
+}
 // the rate tables in one run: sec and upt per (type, species), d and e per species
 size_t table_floats(const glz_adj *h) { return (size_t)2 * h->n_types * h->n_species + 2 * h->n_species; }
 
@@ -455,7 +801,7 @@ int step_forward(glz_adj *h, int t, const float *in, float *out) {
             p.out = p.last ? out + (size_t)s * n : h->tmp[r & 1] + (size_t)s * n;
             if (p.active) cur[s] = p.out;
         }
-        CU(launch_after(forward_round, blocks_for(h), 0, h->stream, a));
+        if (int rc = launch_forward(h, a)) return rc;
     }
     return GLZ_OK;
 }
@@ -487,7 +833,7 @@ int keep_step(glz_adj *h, int sg, int local, int len, float *last_out) {
                 p.out = seg_state(h, sg, local, r + 1, s);
             }
         }
-        CU(launch_after(forward_round, blocks_for(h), 0, h->stream, a));
+        if (int rc = launch_forward(h, a)) return rc;
     }
     return GLZ_OK;
 }
@@ -566,7 +912,12 @@ int backward_sequence(glz_adj *h) {
     a.de = h->d_de;
     a.partial = h->partial;
     const size_t smem = ((size_t)kWarps * 2 * T + G) * sizeof(double);
-    CU(cudaFuncSetAttribute(backward_round, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // owner types held in registers up to 4 or 8 types, else reduced per trip
+    auto *backward = !quads(h) ? backward_round
+                     : T <= 4  ? backward_quads<4>
+                     : T <= 8  ? backward_quads<8>
+                               : backward_quads<0>;
+    CU(cudaFuncSetAttribute(backward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int nseg = (h->steps + h->every - 1) / h->every;
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int t0 = sg * h->every, len = (t0 + h->every < h->steps ? t0 + h->every : h->steps) - t0;
@@ -587,7 +938,7 @@ int backward_sequence(glz_adj *h) {
                     p.lam_in = h->lam[1 - cur[s]] + (size_t)s * sites;
                     cur[s] = 1 - cur[s];
                 }
-                CU(launch_after(backward_round, grid, smem, h->stream, a));
+                CU(launch_after(backward, grid, smem, h->stream, a));
             }
         }
         CU(cudaGetLastError());

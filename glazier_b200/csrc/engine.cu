@@ -1076,13 +1076,15 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     // staging costs more than it saves.
     const long long direct_most_general = g.dim == 2 ? 1024LL * 1024LL : 128LL * 128LL * 128LL;
     h->direct = direct_mode == 1 || (direct_mode == -1 && sites <= (h->lean ? direct_most : direct_most_general));
-    // From a million targets a pass the direct kernel queues each warp's
-    // unlike copies and prices them in full rounds (GLAZIER_SWEEP_COMPACT=1:
-    // at any size, =0: never).
-    // GLAZIER_SWEEP_COMPACT=2: a block-wide queue instead, at any size.
+    // From 2^18 targets a pass the direct kernel gathers each block's unlike
+    // copies into one queue priced by whole warps, and from a million it
+    // queues each warp's (GLAZIER_SWEEP_COMPACT=0: neither, =1: the warp's,
+    // =2: the block's, at any size).
     const char *compact_env = std::getenv("GLAZIER_SWEEP_COMPACT");
     const int compact_mode = compact_env ? (compact_env[0] == '0' ? 0 : (compact_env[0] == '2' ? 2 : 1)) : -1;
-    h->compact = compact_mode >= 0 ? compact_mode : (sites / g.ncol >= glz::kDirectCompactFrom ? 1 : 0);
+    const long long targets = sites / g.ncol;
+    h->compact = compact_mode >= 0 ? compact_mode
+                                   : (targets >= glz::kDirectCompactFrom ? 1 : (targets >= glz::kDirectGatherFrom ? 2 : 0));
     // With no fields, division or death there is nothing between colour
     // passes: a direct plane of at most 512^2 sites runs every MCS of a call
     // in one cooperative launch, which saves more launch time than its grid

@@ -152,7 +152,9 @@ struct ResidentLaunch {
 
 // cudaErrorCooperativeLaunchTooLarge (and nothing launched) when the blocks
 // cannot all be resident at once.
-// Targets a pass from which the direct kernel queues a warp's unlike copies.
+// Targets a pass from which the direct kernel queues a block's unlike copies
+// (kDirectGatherFrom) and from which a warp's (kDirectCompactFrom).
+constexpr int kDirectGatherFrom = 1 << 18;
 constexpr int kDirectCompactFrom = 1 << 20;
 
 cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream);

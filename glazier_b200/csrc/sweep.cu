@@ -1274,17 +1274,17 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access
 // warp's queue, and the warp prices the queue in full rounds, so that a
 // round's lanes all have a copy to price. The queue pays on large passes
 // (0.37 against 0.51 ms per MCS at 256^3 with K 4); below a million targets
-// a pass (kDirectCompactFrom, engine.h) the plain form's four times wider
-// grid hides more latency and is as fast or faster.
+// a pass (kDirectCompactFrom, engine.h) the block-queued form below, with its
+// wider grid, hides more latency.
 constexpr int kDirectCompactK = 4;
 // K < 0: the block's 256 |K| consecutive targets are drawn and compared by
 // all its threads, the unlike ones gathered into one block-wide queue, and
 // the queue priced from its front by as many whole warps as it needs: the
 // plain form's wide grid, with a warp's lanes busy in the pricing rounds.
-#ifndef GLZ_DIRECT_BLOCK_K
-#define GLZ_DIRECT_BLOCK_K 1
-#endif
-constexpr int kDirectBlockK = -GLZ_DIRECT_BLOCK_K;
+// Two targets a thread in a plane, one in a volume (per MCS at 1024^2: 37.3
+// us with two, 52.0 with one; at 128^3: 0.066 ms with one, 0.071 with two).
+template <int DIM>
+constexpr int kDirectBlockK = DIM == 2 ? -2 : -1;
 
 template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
 __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
@@ -1786,7 +1786,7 @@ template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
     const int targets = (a.g.w / 2) * (a.g.h / 2) * (DIM == 3 ? a.g.d / 2 : 1);
     const bool compact = a.compact == 1, gathered = a.compact == 2;
-    const int per_block = 256 * (compact ? kDirectCompactK : (gathered ? -kDirectBlockK : 1));
+    const int per_block = 256 * (compact ? kDirectCompactK : (gathered ? -kDirectBlockK<DIM> : 1));
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)((targets + per_block - 1) / per_block));
     cfg.blockDim = dim3(256);
@@ -1801,18 +1801,18 @@ static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
         cfg.numAttrs = 0;
         if (!a.lean)
             return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
-                   : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK, true>, a)
+                   : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, true>, a)
                               : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, true>, a);
         return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
-               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK, false>, a)
+               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, false>, a)
                           : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, false>, a);
     }
     if (!a.lean)  // every term: length, chemotaxis, connectivity, motility, drift, nematic, moments
         return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
-               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK, true>, a)
+               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, true>, a)
                           : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, true>, a);
     return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
-           : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK, false>, a)
+           : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, false>, a)
                       : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, false>, a);
 }
 

@@ -26,6 +26,9 @@ CASES = {
     "plane": (64, 48, 1, 8, (7, 5, 1), 12, (0.3, 0.1)),
     # D 0.2 takes two sub-steps in 3D (limit 1/6), 0.05 one
     "cube": (16, 16, 12, 4, (4, 4, 2), 7, (0.2, 0.05)),
+    # rows of 66 sites, not a multiple of four: the one-site round kernels
+    # (the cases above take the four-site ones)
+    "odd-rows": (66, 40, 1, 6, (10, 6, 1), 9, (0.3, 0.1)),
 }
 
 
@@ -208,6 +211,43 @@ def test_the_initial_field_gradient_matches_autograd(recorded):
     ((out - target) ** 2).mean().backward()
     auto = f0_64.grad.numpy()
     assert np.abs(gf.cpu().numpy() - auto).max() / np.abs(auto).max() < 1e-4
+
+
+@pytest.mark.parametrize("n_types", [6, 12])
+def test_more_owner_types_give_the_same_gradient(recorded, n_types):
+    """The backward keeps its exchange gradients per owner type in registers
+    for up to 4 or 8 types and reduces them warp by warp past that: the same
+    trajectory declared with unused extra types (their rates zero) gives the
+    same gradient for the rates it uses and exactly zero for the others."""
+    import torch
+
+    from glazier_b200.adjoint import FieldAdjoint
+
+    st, f0, traj, _ = recorded
+    m = st.model
+    target = _target(st, traj, f0)
+    base, gf_base = _device_gradient(st, traj, f0, target, every=4)
+    T, S = m.n_types, 2
+    p = _params(m)
+    sec = np.zeros((n_types, S))
+    upt = np.zeros((n_types, S))
+    sec[:T] = np.asarray(m.secretion, dtype=np.float64)
+    upt[:T] = np.asarray(m.uptake, dtype=np.float64)
+    padded = np.concatenate([p[:2 * S], sec.reshape(-1), upt.reshape(-1)])
+    adj = FieldAdjoint(m.width, m.height, m.depth, S, n_types, traj, checkpoint_every=4)
+    out = adj.forward(padded, torch.from_numpy(f0.astype(np.float32)).cuda())
+    gp, gf = adj.backward(2.0 * (out - target.to(torch.float32).cuda()) / out.numel())
+    adj.close()
+    g_sec = gp[2 * S:2 * S + n_types * S].reshape(n_types, S)
+    g_upt = gp[2 * S + n_types * S:].reshape(n_types, S)
+    want_sec = base[2 * S:2 * S + T * S].reshape(T, S)
+    want_upt = base[2 * S + T * S:].reshape(T, S)
+    scale = np.abs(base).max()
+    assert np.array_equal(gp[:2 * S], base[:2 * S])  # diffusion and decay sum the same way
+    assert np.abs(g_sec[:T] - want_sec).max() <= 1e-12 * scale
+    assert np.abs(g_upt[:T] - want_upt).max() <= 1e-12 * scale
+    assert np.all(g_sec[T:] == 0.0) and np.all(g_upt[T:] == 0.0)
+    assert torch.equal(gf, gf_base)
 
 
 def test_the_autograd_function_carries_the_gradient(recorded):

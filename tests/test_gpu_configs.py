@@ -7,11 +7,12 @@ replay of the schedule (oracle/replay.c) after a first MCS and at the end:
   - the plain monolayer: 128^2, 256 cells of side 8, J=10, lambda_V=1,
     V_t=64, T=10, 100 MCS;
   - the scaling sweep's planes with the surface term (lambda_S=0.2, S_t=92):
-    1024^2 and 4096^2 for 10 MCS each, the latter on the windowed lean
-    kernel's full persistent grid (444 CTAs walking their tiles through
-    their three-stage TMA window rings);
+    1024^2 and 4096^2 for 10 MCS each, the former on the block-queued direct
+    kernel, the latter on the windowed lean kernel's full persistent grid
+    (444 CTAs walking their tiles through their three-stage TMA window
+    rings);
   - the scaling sweep's 128^3 volume, 26 neighbours, lambda_S=0.2,
-    S_t=3176, for 10 MCS;
+    S_t=3176, for 10 MCS, on the block-queued direct kernel;
   - a lean volume just past the size from which the direct kernel queues its
     copies (204^3 sites, 2^20 targets a pass), so the default thresholds are
     held to the replay too.
@@ -64,7 +65,7 @@ def test_the_plain_monolayer_replays_bit_for_bit_over_100_mcs(device):
 def test_the_1024_plane_with_the_surface_term_replays_bit_for_bit(device):
     start = monolayer(1024, lambda_surface=0.2, target_surface=initial_surface(8))
     assert start.model.types[1].target_surface == 92.0
-    _run_both(device, start, 10, "direct")
+    _run_both(device, start, 10, "gathered")
 
 
 def test_the_4096_plane_with_the_surface_term_replays_bit_for_bit(device):
@@ -75,7 +76,7 @@ def test_the_4096_plane_with_the_surface_term_replays_bit_for_bit(device):
 def test_the_128_volume_with_the_surface_term_replays_bit_for_bit(device):
     start = monolayer(128, depth=128, lambda_surface=0.2, target_surface=initial_surface(8, 3))
     assert start.model.types[1].target_surface == 3176.0
-    _run_both(device, start, 10, "direct")
+    _run_both(device, start, 10, "gathered")
 
 
 def test_a_volume_past_the_queueing_threshold_replays_bit_for_bit(device):
