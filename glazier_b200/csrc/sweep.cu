@@ -1281,10 +1281,17 @@ constexpr int kDirectCompactK = 4;
 // all its threads, the unlike ones gathered into one block-wide queue, and
 // the queue priced from its front by as many whole warps as it needs: the
 // plain form's wide grid, with a warp's lanes busy in the pricing rounds.
-// Two targets a thread in a plane, one in a volume (per MCS at 1024^2: 37.3
-// us with two, 52.0 with one; at 128^3: 0.066 ms with one, 0.071 with two).
+// Two targets a thread (per MCS at 1024^2: 37.3 us with two, 52.0 with one;
+// at 128^3, with the register cap below, 0.060 ms with two, 0.062 with one).
 template <int DIM>
-constexpr int kDirectBlockK = DIM == 2 ? -2 : -1;
+constexpr int kDirectBlockK = -2;
+
+// Direct passes of the lean models are held to 64 registers, four blocks of
+// 256 per SM, so that a 2^18-target pass of two targets a thread is one wave
+// (at 128^3: 0.060 ms per MCS against 0.073 uncapped, 0.065 at 48 registers);
+// the every-term passes keep their registers (capped, they spill and slow).
+template <bool EXTRAS>
+constexpr int kDirectMinBlocks = EXTRAS ? 1 : 4;
 
 template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
 __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
@@ -1393,7 +1400,7 @@ __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
 }
 
 template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
-__global__ void __launch_bounds__(256) direct_sweep_kernel(const __grid_constant__ SweepLaunch a) {
+__global__ void __launch_bounds__(256, kDirectMinBlocks<EXTRAS>) direct_sweep_kernel(const __grid_constant__ SweepLaunch a) {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     direct_sweep_body<DIM, NOFF, UNIFORM, K, EXTRAS>(a);
@@ -1425,7 +1432,7 @@ __device__ __forceinline__ void clock_patch(SweepLaunch &d) {
 // The direct pass of a step replayed from a graph: the block copies the
 // launch into shared memory, patches it from the clock and prices from there.
 template <int DIM, int NOFF, bool UNIFORM, int K, bool EXTRAS>
-__global__ void __launch_bounds__(256) direct_sweep_clocked(const __grid_constant__ SweepLaunch a) {
+__global__ void __launch_bounds__(256, kDirectMinBlocks<EXTRAS>) direct_sweep_clocked(const __grid_constant__ SweepLaunch a) {
     __shared__ SweepLaunch d;
     static_assert(sizeof(SweepLaunch) % sizeof(int) == 0, "the launch copies as words");
     const int *src = reinterpret_cast<const int *>(&a);
