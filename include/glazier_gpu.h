@@ -165,10 +165,10 @@ uint64_t glz_gpu_mcs(const glz_gpu *h);
 size_t glz_gpu_n_labels(const glz_gpu *h);
 
 /* The sweep kernel the handle's next step takes: "band", "lean", "direct",
- * "compact", "resident", "cluster" or "general" (the engine picks it from
- * the model's terms and the lattice's size; "direct" and "compact" take
- * every term, "band", "lean", "resident" and "cluster" contact, volume and
- * surface only, "general" every term through tiles). A diagnostic with no reference
+ * "gathered", "compact", "resident", "cluster" or "general" (the engine picks
+ * it from the model's terms and the lattice's size; "direct", "gathered" and
+ * "compact" take every term, "band", "lean", "resident" and "cluster"
+ * contact, volume and surface only, "general" every term through tiles). A diagnostic with no reference
  * counterpart: the reference has one kernel (lib.rs:436-716). Never NULL. */
 const char *glz_gpu_sweep_kernel(const glz_gpu *h);
 
