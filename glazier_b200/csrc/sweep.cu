@@ -1585,18 +1585,36 @@ cudaError_t launch_resident_sweep(const ResidentLaunch &r, cudaStream_t stream) 
 // the lattice and tallies go back to global memory at the end.
 
 constexpr int kClusterThreads = 1024;
-constexpr int kClusterMax = 16;
+#ifndef GLZ_CLUSTER_MAX
+#define GLZ_CLUSTER_MAX 16
+#endif
+constexpr int kClusterMax = GLZ_CLUSTER_MAX;  // CTAs of a cluster at most (16 is the non-portable limit)
+// A plane takes a cluster of at least kClusterMin CTAs (fewer only when it
+// has fewer rows), more while a CTA would hold more targets than threads:
+// a pass's work per CTA is what bounds it, so spreading a 128^2 plane over
+// 8 SMs rather than 4 cuts its 100 MCS from 1.17 to 0.99 ms.
+#ifndef GLZ_CLUSTER_MIN
+#define GLZ_CLUSTER_MIN 8
+#endif
+constexpr int kClusterMin = GLZ_CLUSTER_MIN;  // a power of two
 constexpr int kClusterSmem = 200 * 1024;
+#ifndef GLZ_CLUSTER_PER_THREAD
+#define GLZ_CLUSTER_PER_THREAD 1
+#endif
+constexpr int kClusterPerThread = GLZ_CLUSTER_PER_THREAD;  // a pass's targets a thread draws at most
 
 // Shared-memory layout of one CTA of a C-CTA cluster sweep (bytes from the
 // start): delta[3][Lc] (i64), base[2][Lc] (int2), the pointer tables
-// (delta 3C, base 2C, volc C), rows[H], slab[R W] (u32), volc[Lc][4] (i32).
+// (delta 3C, base 2C, volc C), rows[H], slab[R W] (u32), volc[Lc][4] (i32),
+// the pass's queue of unlike copies (target index, pick) with room for every
+// target of the CTA's rows, and the queue's two fill counters.
 struct ClusterLayout {
-    int C, R, Lc;
-    size_t delta, base, dptr, bptr, vptr, rows, slab, volc, bytes;
+    int C, R, Lc, qcap;
+    size_t delta, base, dptr, bptr, vptr, rows, slab, volc, queue, picks, qn, bytes;
     __host__ __device__ ClusterLayout(int w, int h, int n_labels, int c) : C(c) {
         R = (h + c - 1) / c;
         Lc = (n_labels + c - 1) / c;
+        qcap = (R + 1) / 2 * (w / 2);
         delta = 0;
         base = delta + 3 * (size_t)Lc * 8;
         dptr = base + 2 * (size_t)Lc * 8;
@@ -1605,7 +1623,10 @@ struct ClusterLayout {
         rows = vptr + (size_t)c * 8;
         slab = rows + (size_t)h * 8;
         volc = slab + ((size_t)R * w * 4 + 15) / 16 * 16;
-        bytes = volc + (size_t)Lc * 16;
+        queue = volc + (size_t)Lc * 16;
+        picks = queue + (size_t)qcap * 4;
+        qn = picks + ((size_t)qcap + 15) / 16 * 16;
+        bytes = qn + 16;
     }
 };
 
@@ -1653,7 +1674,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) cluster_sweep_kernel(const
     uint32_t **rows = reinterpret_cast<uint32_t **>(smem_raw + L.rows);
     uint32_t *slab = reinterpret_cast<uint32_t *>(smem_raw + L.slab);
     int *volc = reinterpret_cast<int *>(smem_raw + L.volc);
+    int *queue = reinterpret_cast<int *>(smem_raw + L.queue);
+    uint8_t *picks = reinterpret_cast<uint8_t *>(smem_raw + L.picks);
+    int *qn = reinterpret_cast<int *>(smem_raw + L.qn);
     const int y0 = rank * L.R, y1 = min(H, y0 + L.R);
+    const int lane = tid & 31;
+    if (tid < 2) qn[tid] = 0;
 
     // this CTA's rows and labels, and where every CTA's parts lie
     for (int i = tid; i < (y1 - y0) * W; i += nth) slab[i] = a.labels[(size_t)y0 * W + i];
@@ -1683,12 +1709,45 @@ __global__ void __launch_bounds__(kClusterThreads, 1) cluster_sweep_kernel(const
             const ClusterPass acc{rows, bptr, dptr, vptr, C, __ffs(C) - 1, C - 1, c,
                                   (int)(p % 2), (int)((p + 2) % 3), (int)(p % 3)};
             const uint64_t key_pick = stream_key(r.seed, step, c, 0), key_accept = stream_key(r.seed, step, c, 1);
-            // this CTA's targets of colour c: rows of its slab of the colour's parity
+            // this CTA's targets of colour c: rows of its slab of the colour's
+            // parity. Every thread draws its targets' picks and compares the
+            // two labels; the unlike ones go into the CTA's queue (a warp's
+            // slots reserved at once), which whole warps then price from its
+            // front. A pass's copies read only its snapshot and other
+            // colours' labels and commit by atomics, so the queue's order
+            // changes nothing.
             const int yf = y0 + ((y0 & 1) != ((c >> 1) & 1));
             const int count = yf < y1 ? (y1 - yf + 1) / 2 * hw : 0;
-            for (int t = tid; t < count; t += nth) {
+            int *fill = qn + (p & 1);
+            for (int t0 = 0; t0 < count; t0 += nth) {
+                const int t = t0 + tid;
+                bool unlike = false;
+                int pick = 0;
+                if (t < count) {
+                    const int y = yf + 2 * (t / hw), x = 2 * (t % hw) + (c & 1);
+                    pick = pick_of<NOFF>(draw(key_pick, (uint32_t)(y * W + x)));
+                    int dx, dy, dz;
+                    pick_offset<2, NOFF>(pick, dx, dy, dz);
+                    const int nx = x + dx < 0 ? W - 1 : (x + dx >= W ? 0 : x + dx);
+                    const int ny = y + dy < 0 ? H - 1 : (y + dy >= H ? 0 : y + dy);
+                    unlike = acc.label(x, y, 0) != acc.label(nx, ny, 0);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, unlike);
+                int slot = 0;
+                if (lane == 0 && m) slot = atomicAdd(fill, __popc(m));
+                slot = __shfl_sync(0xffffffffu, slot, 0) + __popc(m & ((1u << lane) - 1u));
+                if (unlike) {
+                    queue[slot] = t;
+                    picks[slot] = (uint8_t)pick;
+                }
+            }
+            __syncthreads();
+            const int total = *fill;
+            if (tid == 0) qn[(p + 1) & 1] = 0;  // the next pass's counter; no thread reads it before the cluster barrier
+            for (int e = tid; e < total; e += nth) {
+                const int t = queue[e];
                 const int y = yf + 2 * (t / hw), x = 2 * (t % hw) + (c & 1);
-                direct_target<2, NOFF, UNIFORM>(a, acc, key_pick, key_accept, x, y, 0);
+                direct_target<2, NOFF, UNIFORM>(a, acc, key_pick, key_accept, x, y, 0, (int)picks[e]);
             }
             // this CTA's labels' rotation for the next pass, which no thread of this one reads
             int2 *next_base = base + ((p + 1) % 2) * L.Lc;
@@ -1721,11 +1780,11 @@ template <int NOFF, bool UNIFORM>
 static cudaError_t launch_cluster(const ResidentLaunch &r, cudaStream_t stream) {
     const SweepLaunch &a = r.a;
     const long long targets = (long long)a.g.w * a.g.h / 4;
-    int want = 1;
+    int want = kClusterMin;
     while (want < kClusterMax && (long long)want * kClusterThreads < targets) want *= 2;
-    // a thread's targets price one after another: past one each the
-    // cooperative grid's wider spread is faster
-    if ((long long)want * kClusterThreads < targets) return cudaErrorNotSupported;
+    // past kClusterPerThread targets a thread the cooperative grid's wider
+    // spread is faster
+    if ((long long)want * kClusterThreads * kClusterPerThread < targets) return cudaErrorNotSupported;
     auto kernel = cluster_sweep_kernel<NOFF, UNIFORM>;
     static bool ready = false;
     if (!ready) {
