@@ -31,6 +31,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "device.cuh"
 #include "engine.h"
 #include "neighbours.cuh"
@@ -513,13 +515,17 @@ static bool band_shape(int w, int h, int smem_budget, int &seg, int &slots, int 
 
 template <int NOFF, bool UNIFORM>
 static cudaError_t launch_band(const ResidentLaunch &r, cudaStream_t stream) {
-    static int sms = 0, optin = 0;
-    if (!sms) {
-        int dev = 0;
+    // the SM count and shared-memory budget, looked up once (handles on other
+    // host threads may launch too)
+    static std::atomic<int> sms_once{0}, optin_once{0};
+    if (!sms_once.load(std::memory_order_acquire)) {
+        int dev = 0, n = 0;
         if (cudaError_t e = cudaGetDevice(&dev)) return e;
-        if (cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return e;
-        optin = band_budget(dev);
+        if (cudaError_t e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev)) return e;
+        optin_once.store(band_budget(dev), std::memory_order_relaxed);
+        sms_once.store(n, std::memory_order_release);
     }
+    const int sms = sms_once.load(std::memory_order_acquire), optin = optin_once.load(std::memory_order_relaxed);
     BandLaunch b{};
     b.r = r;
     size_t smem = 0;

@@ -25,6 +25,7 @@
 // a host replay of the same schedule reproduces it bit for bit.
 
 #include <cooperative_groups.h>
+#include <atomic>
 #include <cuda.h>
 
 #include <cstdlib>
@@ -1531,16 +1532,17 @@ template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch_resident(const ResidentLaunch &r, cudaStream_t stream) {
     const int targets = (r.a.g.w / 2) * (r.a.g.h / 2) * (DIM == 3 ? r.a.g.d / 2 : 1);
     const int blocks = (targets + 255) / 256;
-    static int most = 0;
-    if (!most) {
+    static std::atomic<int> most_once{0};  // handles on other host threads may launch too
+    if (!most_once.load(std::memory_order_acquire)) {
         int dev = 0, sms = 0, per_sm = 0;
         if (cudaError_t e = cudaGetDevice(&dev)) return e;
         if (cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return e;
         if (cudaError_t e =
                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, resident_sweep_kernel<DIM, NOFF, UNIFORM>, 256, 0))
             return e;
-        most = sms * per_sm;
+        most_once.store(sms * per_sm, std::memory_order_release);
     }
+    const int most = most_once.load(std::memory_order_acquire);
     if (blocks > most) return cudaErrorCooperativeLaunchTooLarge;
     void *args[] = {const_cast<ResidentLaunch *>(&r)};
     return cudaLaunchCooperativeKernel((const void *)resident_sweep_kernel<DIM, NOFF, UNIFORM>, dim3(blocks), dim3(256),
@@ -1786,14 +1788,14 @@ static cudaError_t launch_cluster(const ResidentLaunch &r, cudaStream_t stream) 
     // spread is faster
     if ((long long)want * kClusterThreads * kClusterPerThread < targets) return cudaErrorNotSupported;
     auto kernel = cluster_sweep_kernel<NOFF, UNIFORM>;
-    static bool ready = false;
-    if (!ready) {
+    static std::atomic<bool> ready{false};  // handles on other host threads may launch too
+    if (!ready.load(std::memory_order_acquire)) {
         if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmem) ||
             cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) {
             cudaGetLastError();
             return cudaErrorNotSupported;
         }
-        ready = true;
+        ready.store(true, std::memory_order_release);
     }
     // the widest cluster up to `want` CTAs that the device schedules and whose parts fit
     for (int C = want; C >= 1; C /= 2) {
@@ -1885,9 +1887,9 @@ static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
 template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cudaStream_t stream) {
     using T = Tile<DIM>;
-    static int grid_cap = 0;
+    static std::atomic<int> grid_cap_once{0};  // handles on other host threads may launch too
     const size_t smem = sizeof(LeanSmem<DIM>) + 128;
-    if (!grid_cap) {
+    if (!grid_cap_once.load(std::memory_order_acquire)) {
         cudaError_t e = cudaFuncSetAttribute(lean_sweep_kernel<DIM, NOFF, UNIFORM>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e) return e;
@@ -1897,10 +1899,11 @@ static cudaError_t launch_lean(const SweepLaunch &a, const CUtensorMap &tmap, cu
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lean_sweep_kernel<DIM, NOFF, UNIFORM>,
                                                                kLeanThreads, smem)))
             return e;
-        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
+        grid_cap_once.store(sms * (per_sm > 0 ? per_sm : 1), std::memory_order_release);
     }
     const int tiles = ((a.g.w + T::TX - 1) / T::TX) * ((a.g.h + T::TY - 1) / T::TY) *
                       (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
+    const int grid_cap = grid_cap_once.load(std::memory_order_acquire);
     int grid = tiles < grid_cap ? tiles : grid_cap;
     if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
     // Programmatic launch: the grid may start its prologue while the previous
@@ -1933,9 +1936,9 @@ static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
     if (a.direct) return launch_direct<DIM, NOFF, UNIFORM>(a, stream);
     if (a.lean) return launch_lean<DIM, NOFF, UNIFORM>(a, tmap, stream);
     using T = Tile<DIM>;
-    static int grid_cap = 0;
+    static std::atomic<int> grid_cap_once{0};  // handles on other host threads may launch too
     const size_t smem = sizeof(SweepSmem<DIM>) + 128;
-    if (!grid_cap) {
+    if (!grid_cap_once.load(std::memory_order_acquire)) {
         cudaError_t e = cudaFuncSetAttribute(sweep_kernel<DIM, NOFF, UNIFORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e) return e;
@@ -1944,10 +1947,11 @@ static cudaError_t launch(const SweepLaunch &a, cudaStream_t stream) {
         if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))) return e;
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<DIM, NOFF, UNIFORM>, kThreads, smem)))
             return e;
-        grid_cap = sms * (per_sm > 0 ? per_sm : 1);
+        grid_cap_once.store(sms * (per_sm > 0 ? per_sm : 1), std::memory_order_release);
     }
     const int tiles = ((a.g.w + T::TX - 1) / T::TX) * ((a.g.h + T::TY - 1) / T::TY) *
                       (DIM == 3 ? (a.g.d + T::TZ - 1) / T::TZ : 1);
+    const int grid_cap = grid_cap_once.load(std::memory_order_acquire);
     int grid = tiles < grid_cap ? tiles : grid_cap;
     if (a.max_ctas > 0 && grid > a.max_ctas) grid = a.max_ctas;
     // programmatic launch as the lean kernel's, except for a motility pass,
@@ -2512,16 +2516,17 @@ static cudaError_t direct_ensemble_shape(const EnsembleLaunch &e, cudaStream_t s
         direct_ensemble_kernel<NOFF, UNIFORM, BX, BY><<<e.total_tiles, BX * BY, 0, stream>>>(e);
         return cudaGetLastError();
     }
-    static int most = 0;  // blocks that can all be resident at once
-    if (!most) {
+    static std::atomic<int> most_once{0};  // blocks that can all be resident at once
+    if (!most_once.load(std::memory_order_acquire)) {
         int dev = 0, sms = 0, per_sm = 0;
         if (cudaError_t x = cudaGetDevice(&dev)) return x;
         if (cudaError_t x = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return x;
         if (cudaError_t x = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                 &per_sm, direct_ensemble_step_kernel<NOFF, UNIFORM, BX, BY>, BX * BY, 0))
             return x;
-        most = sms * per_sm;
+        most_once.store(sms * per_sm, std::memory_order_release);
     }
+    const int most = most_once.load(std::memory_order_acquire);
     if (most < 1) return cudaErrorCooperativeLaunchTooLarge;
     const int grid = e.total_tiles < most ? e.total_tiles : most;
     if (cudaError_t x = cudaMemsetAsync(e.barrier, 0, 2 * sizeof(unsigned), stream)) return x;
@@ -2545,8 +2550,8 @@ __global__ void clock_advance_kernel(EnsembleClock *clock, int ncol) {
 
 template <int DIM, int NOFF, bool UNIFORM>
 static int ensemble_cap() {
-    static int cap = 0;
-    if (!cap) {
+    static std::atomic<int> cap{0};  // handles on other host threads may launch too
+    if (!cap.load(std::memory_order_acquire)) {
         const size_t smem = sizeof(EnsembleSmem<DIM>) + 128;
         if (cudaFuncSetAttribute(ensemble_sweep_kernel<DIM, NOFF, UNIFORM>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))
@@ -2556,9 +2561,9 @@ static int ensemble_cap() {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_sweep_kernel<DIM, NOFF, UNIFORM>, kThreads,
                                                           smem))
             return 0;
-        cap = sms * (per_sm > 0 ? per_sm : 1);
+        cap.store(sms * (per_sm > 0 ? per_sm : 1), std::memory_order_release);
     }
-    return cap;
+    return cap.load(std::memory_order_acquire);
 }
 
 // Whether ensembles take the lean kernel (GLAZIER_ENSEMBLE_LEAN=0: the
@@ -2573,8 +2578,8 @@ static bool lean_ensemble() {
 
 template <int DIM, int NOFF, bool UNIFORM>
 static int lean_ensemble_cap() {
-    static int cap = 0;
-    if (!cap) {
+    static std::atomic<int> cap{0};  // handles on other host threads may launch too
+    if (!cap.load(std::memory_order_acquire)) {
         const size_t smem = sizeof(LeanEnsembleSmem<DIM>) + 128;
         if (cudaFuncSetAttribute(lean_ensemble_kernel<DIM, NOFF, UNIFORM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem))
@@ -2584,9 +2589,9 @@ static int lean_ensemble_cap() {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lean_ensemble_kernel<DIM, NOFF, UNIFORM>,
                                                           kLeanThreads, smem))
             return 0;
-        cap = sms * (per_sm > 0 ? per_sm : 1);
+        cap.store(sms * (per_sm > 0 ? per_sm : 1), std::memory_order_release);
     }
-    return cap;
+    return cap.load(std::memory_order_acquire);
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
