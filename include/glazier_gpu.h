@@ -12,7 +12,8 @@
  *     glz_last_error() returns for the calling thread.
  *   - One handle owns one CUDA stream on one device. A handle is not safe to
  *     use from two threads at once (the reference `GpuSession` is
- *     `unsendable`); distinct handles are independent.
+ *     `unsendable`); distinct handles are independent and may be driven
+ *     from host threads of their own at the same time.
  *   - A model input the device engine would not use (an activity field with
  *     no motility term) is refused at creation with GLZ_UNSUPPORTED, never
  *     dropped silently (lib.rs:819-821).
