@@ -27,7 +27,7 @@ def _alone(device, start, steps):
     return out
 
 
-@pytest.mark.parametrize("size", [128, 512, 1024, 2048])
+@pytest.mark.parametrize("size", [128, 512, 1024, 2048, 4096])
 def test_two_handles_on_two_threads_each_run_as_alone(device, size):
     start = monolayer(size, lambda_surface=0.2, target_surface=initial_surface(8))
     steps = 6
