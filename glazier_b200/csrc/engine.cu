@@ -1060,16 +1060,18 @@ int glz_gpu_create(const glz_model *m, const uint32_t *labels, const uint8_t *ce
     const char *lean_env = std::getenv("GLAZIER_SWEEP_LEAN");
     h->lean = !h->has_length && !h->tracks && !h->has_chemotaxis && !h->has_external && !h->has_motility && !has_conn &&
               !(lean_env && lean_env[0] == '0');
-    // A lean plane of at most 2048^2 sites, or a lean volume of any size,
-    // takes the direct kernel: reading the lattice through the caches beats
-    // the lean kernel's window ring there (per MCS, L2 flushed: 0.035 against
-    // 0.040 ms at 1024^2; at 2048^2 the warp-queued form's pass 14.8 against
-    // 15.7 us; 0.37 against 0.91 ms at 256^3 and 0.64 against 1.07 ms at
-    // 320^3, a lattice past L2; at 4096^2 the lean kernel leads, 0.144
-    // against 0.164 ms). GLAZIER_SWEEP_DIRECT=0: never, =1: at any size.
+    // A lean plane of at most 1024^2 sites, or a lean volume of any size,
+    // takes the direct kernel: one thread per target reading the lattice
+    // through the caches beats the lean kernel's window ring there (per MCS,
+    // L2 flushed: 0.035 against 0.040 ms at 1024^2; 0.37 against 0.91 ms at
+    // 256^3 and 0.64 against 1.07 ms at 320^3, a lattice past L2; at 2048^2
+    // and 4096^2 the lean kernel leads: 100 MCS back to back at 2048^2 take
+    // 5.8 ms on it against 7.8 ms on the warp-queued direct kernel, though a
+    // single MCS after an L2 flush is 6 % faster on the latter).
+    // GLAZIER_SWEEP_DIRECT=0: never, =1: at any size.
     const char *direct_env = std::getenv("GLAZIER_SWEEP_DIRECT");
     const int direct_mode = direct_env ? (direct_env[0] == '0' ? 0 : 1) : -1;
-    const long long direct_most = g.dim == 2 ? 2048LL * 2048LL : sites;
+    const long long direct_most = g.dim == 2 ? 1024LL * 1024LL : sites;
     // Models with other terms (length, chemotaxis, connectivity, motility,
     // drift, nematic, division and death) take the direct kernel on planes up
     // to 1024^2 and volumes up to 128^3, where the tiled kernel's window

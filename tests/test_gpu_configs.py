@@ -10,7 +10,7 @@ replay of the schedule (oracle/replay.c) after a first MCS and at the end:
     1024^2 and 4096^2 for 10 MCS each, the former on the block-queued direct
     kernel, the latter on the windowed lean kernel's full persistent grid
     (444 CTAs walking their tiles through their three-stage TMA window
-    rings), and 2048^2 for 4 MCS on the warp-queued direct kernel;
+    rings), and 2048^2 for 4 MCS on the lean kernel with 2.3 tiles a CTA;
   - the scaling sweep's 128^3 volume, 26 neighbours, lambda_S=0.2,
     S_t=3176, for 10 MCS, on the block-queued direct kernel;
   - a lean volume just past the size from which the direct kernel queues its
@@ -68,9 +68,9 @@ def test_the_1024_plane_with_the_surface_term_replays_bit_for_bit(device):
     _run_both(device, start, 10, "gathered")
 
 
-def test_the_2048_plane_replays_bit_for_bit_on_the_warp_queued_direct_kernel(device):
+def test_the_2048_plane_replays_bit_for_bit_on_the_lean_kernel(device):
     start = monolayer(2048, lambda_surface=0.2, target_surface=initial_surface(8))
-    _run_both(device, start, 4, "compact")
+    _run_both(device, start, 4, "lean")
 
 
 def test_the_4096_plane_with_the_surface_term_replays_bit_for_bit(device):
