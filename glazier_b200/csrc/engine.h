@@ -123,6 +123,7 @@ struct SweepLaunch {
     int lean;                // take the lean kernel: no length, chemotaxis, connectivity or moment tracking
     int direct;              // a lean model small enough for the direct kernel (one thread per target)
     int compact;             // the direct kernel queues unlike copies before pricing them: 1 per warp, 2 per block
+    int direct_span;         // targets a block of the block-queued direct kernel takes (0: 256 a thread-row)
     int max_ctas;            // > 0 caps the persistent grid (each CTA then walks more tiles)
     const void *tensor_map;  // CUtensorMap in device-visible memory, or null
     int *error_flag;

@@ -1194,7 +1194,9 @@ __device__ __forceinline__ void pick_offset(int pick, int &dx, int &dy, int &dz)
 // operation for operation.
 template <int DIM, int NOFF, bool UNIFORM, class Access, bool EXTRAS = false>
 __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access &acc, uint64_t key_pick,
-                                              uint64_t key_accept, int x, int y, int z, int known_pick = -1) {
+                                              uint64_t key_accept, int x, int y, int z, int known_pick = -1,
+                                              bool known_labels = false, uint32_t known_old = 0,
+                                              uint32_t known_new = 0) {
     const int W = a.g.w, H = a.g.h, D = a.g.d;
     const int xm = x == 0 ? W - 1 : x - 1, xp = x == W - 1 ? 0 : x + 1;
     const int ym = y == 0 ? H - 1 : y - 1, yp = y == H - 1 ? 0 : y + 1;
@@ -1210,9 +1212,13 @@ __device__ __forceinline__ void direct_target(const SweepLaunch &a, const Access
     const int pick = known_pick >= 0 ? known_pick : pick_of<NOFF>(draw(key_pick, target));
     int dx, dy, dz;
     pick_offset<DIM, NOFF>(pick, dx, dy, dz);
-    const uint32_t nw = acc.label(dx < 0 ? xm : (dx > 0 ? xp : x), dy < 0 ? ym : (dy > 0 ? yp : y),
-                                  dz < 0 ? zm : (dz > 0 ? zp : z));
-    const uint32_t old = acc.label(x, y, z);
+    // A caller that read the two labels earlier in the pass passes them: the
+    // target's changes only by its own commit and the neighbour is another
+    // colour, so they are still the pass's.
+    const uint32_t nw = known_labels ? known_new
+                                     : acc.label(dx < 0 ? xm : (dx > 0 ? xp : x), dy < 0 ? ym : (dy > 0 ? yp : y),
+                                                 dz < 0 ? zm : (dz > 0 ? zp : z));
+    const uint32_t old = known_labels ? known_old : acc.label(x, y, z);
     if (old == nw) return;
     const int2 base_old = acc.base(old), base_new = acc.base(nw);
     const long long prev_old = acc.prev(old), prev_new = acc.prev(nw);
@@ -1310,19 +1316,27 @@ __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
         constexpr int KB = -K;
         __shared__ int queue[256 * KB];
         __shared__ uint8_t picks[256 * KB];
+        __shared__ uint2 pair[256 * KB];  // (old, new) labels of each queued copy, as the light step read them
         __shared__ int counts[8];
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const unsigned below = (1u << lane) - 1u;
-        const int first = blockIdx.x * 256 * KB;
+        // The block's targets [first, last): direct_span of them (at most 256 KB)
+        // when the launch spreads the pass evenly over the SMs' resident
+        // blocks, else 256 KB.
+        const int span = a.direct_span > 0 ? a.direct_span : 256 * KB;
+        const int first = (int)blockIdx.x * span;
+        const int last = min(first + span, targets);
         unsigned masks[KB];
         int picked[KB];
+        uint2 labels[KB];
         int mine = 0;
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
             const int j = first + k * 256 + (int)threadIdx.x;
             bool unlike = false;
             int pick = 0;
-            if (j < targets) {
+            labels[k] = make_uint2(0u, 0u);
+            if (j < last) {
                 int x, y, z;
                 direct_site<DIM>(a, a.colour, j, x, y, z);
                 pick = pick_of<NOFF>(draw(v.key_pick, (uint32_t)((z * a.g.h + y) * a.g.w + x)));
@@ -1331,7 +1345,8 @@ __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
                 const int nx = x + dx < 0 ? a.g.w - 1 : (x + dx >= a.g.w ? 0 : x + dx);
                 const int ny = y + dy < 0 ? a.g.h - 1 : (y + dy >= a.g.h ? 0 : y + dy);
                 const int nz = z + dz < 0 ? a.g.d - 1 : (z + dz >= a.g.d ? 0 : z + dz);
-                unlike = acc.label(x, y, z) != acc.label(nx, ny, nz);
+                labels[k] = make_uint2(acc.label(x, y, z), acc.label(nx, ny, nz));
+                unlike = labels[k].x != labels[k].y;
             }
             masks[k] = __ballot_sync(0xffffffffu, unlike);
             picked[k] = pick;
@@ -1350,6 +1365,7 @@ __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
             if (masks[k] & (1u << lane)) {
                 queue[at + __popc(masks[k] & below)] = first + k * 256 + (int)threadIdx.x;
                 picks[at + __popc(masks[k] & below)] = (uint8_t)picked[k];
+                pair[at + __popc(masks[k] & below)] = labels[k];
             }
             at += __popc(masks[k]);
         }
@@ -1357,7 +1373,9 @@ __device__ __forceinline__ void direct_sweep_body(const SweepLaunch &a) {
         for (int e = (int)threadIdx.x; e < total; e += 256) {
             int x, y, z;
             direct_site<DIM>(a, a.colour, queue[e], x, y, z);
-            direct_target<DIM, NOFF, UNIFORM, GlobalPass, EXTRAS>(a, acc, v.key_pick, v.key_accept, x, y, z, picks[e]);
+            const uint2 ln = pair[e];
+            direct_target<DIM, NOFF, UNIFORM, GlobalPass, EXTRAS>(a, acc, v.key_pick, v.key_accept, x, y, z, picks[e],
+                                                                  true, ln.x, ln.y);
         }
     } else {
         __shared__ int queue[8][32 * K];
@@ -1850,13 +1868,47 @@ static int programmatic_launch() {
     return on;
 }
 
+// Blocks of the block-queued direct kernel that the device holds at once by
+// its launch bounds (SMs x kDirectMinBlocks blocks of 256 threads; the lean
+// form's 64-register cap makes that exactly four per SM); 0 if the SM count
+// cannot be read. A device attribute only, so a launch being captured into
+// a graph may ask.
+static int gathered_slots(bool extras) {
+    static std::atomic<int> sms_once{0};  // handles on other host threads may launch too
+    int sms = sms_once.load(std::memory_order_acquire);
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) {
+            cudaGetLastError();
+            return 0;
+        }
+        sms_once.store(sms, std::memory_order_release);
+    }
+    return sms * (extras ? kDirectMinBlocks<true> : kDirectMinBlocks<false>);
+}
+
 template <int DIM, int NOFF, bool UNIFORM>
 static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
     const int targets = (a.g.w / 2) * (a.g.h / 2) * (DIM == 3 ? a.g.d / 2 : 1);
     const bool compact = a.compact == 1, gathered = a.compact == 2;
     const int per_block = 256 * (compact ? kDirectCompactK : (gathered ? -kDirectBlockK<DIM> : 1));
+    int grid = (targets + per_block - 1) / per_block;
+    SweepLaunch b = a;
+    b.direct_span = 0;
+    if (gathered) {
+        // Spread the pass evenly over whole waves of resident blocks, so that
+        // no SM holds more of its targets than another (at 128^3 and 1024^2:
+        // 592 blocks of 443 targets instead of 512 of 512 on 148 SMs).
+        const int slots = gathered_slots(!a.lean);
+        if (slots > 0) {
+            const int waves = (grid + slots - 1) / slots;
+            const int spread = waves * slots;
+            b.direct_span = (targets + spread - 1) / spread;
+            grid = (targets + b.direct_span - 1) / b.direct_span;
+        }
+    }
     cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3((unsigned)((targets + per_block - 1) / per_block));
+    cfg.gridDim = dim3((unsigned)grid);
     cfg.blockDim = dim3(256);
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
@@ -1868,20 +1920,20 @@ static cudaError_t launch_direct(const SweepLaunch &a, cudaStream_t stream) {
     if (a.clock) {  // a step captured into a graph: plain launches, pass fields from the clock
         cfg.numAttrs = 0;
         if (!a.lean)
-            return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
-                   : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, true>, a)
-                              : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, true>, a);
-        return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
-               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, false>, a)
-                          : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, false>, a);
+            return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, true>, b)
+                   : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, true>, b)
+                              : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, true>, b);
+        return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectCompactK, false>, b)
+               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, false>, b)
+                          : cudaLaunchKernelEx(&cfg, direct_sweep_clocked<DIM, NOFF, UNIFORM, 0, false>, b);
     }
     if (!a.lean)  // every term: length, chemotaxis, connectivity, motility, drift, nematic, moments
-        return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, true>, a)
-               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, true>, a)
-                          : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, true>, a);
-    return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, false>, a)
-           : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, false>, a)
-                      : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, false>, a);
+        return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, true>, b)
+               : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, true>, b)
+                          : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, true>, b);
+    return compact    ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectCompactK, false>, b)
+           : gathered ? cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, kDirectBlockK<DIM>, false>, b)
+                      : cudaLaunchKernelEx(&cfg, direct_sweep_kernel<DIM, NOFF, UNIFORM, 0, false>, b);
 }
 
 template <int DIM, int NOFF, bool UNIFORM>
