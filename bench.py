@@ -49,6 +49,11 @@ BYTES_PER_SITE_UPDATE = 20  # 4 colour passes x 4 B label read + 4 B label write
 METRIC = "site-updates/s (plain 2D sweep, 4096^2)"
 
 
+def metric_for(size: int) -> str:
+    """The metric's name for a plane of `size`^2 (the default is the 4096^2 plane)."""
+    return METRIC.replace("4096^2", f"{size}^2")
+
+
 def workload(size: int):
     from glazier_b200.blueprint import CellType, Model, Start
 
@@ -531,7 +536,7 @@ def run_reference(args) -> None:
     total = per_step * args.steps * cores
     value = total / wall
     line = {
-        "metric": METRIC, "value": value, "unit": "site-updates/s", "impl": "reference", "n_gpus": args.gpus,
+        "metric": metric_for(args.size), "value": value, "unit": "site-updates/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(args.size, args.gpus),
@@ -691,7 +696,7 @@ def run_ours(args) -> None:
     if rank != 0:
         return
     line = {
-        "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_for(args.size), "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": value / PUBLISHED_4096, "dtype": "f32", "data": "synthetic",
         "config": config_dict(args.size, world),
