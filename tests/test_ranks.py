@@ -85,3 +85,11 @@ def test_the_reference_arm_runs_on_rank_zero_alone(monkeypatch):
     with contextlib.redirect_stdout(buf):
         bench.run_reference(args)
     assert buf.getvalue() == ""
+
+
+def test_the_metric_names_the_plane_it_ran():
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    assert bench.metric_for(4096) == bench.METRIC
+    assert bench.metric_for(128) == "site-updates/s (plain 2D sweep, 128^2)"
